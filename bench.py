@@ -1,0 +1,400 @@
+#!/usr/bin/env python3
+"""Benchmark of the fused ZODA column extension on B200.
+
+One step = one fused extension of a full data square that is already
+resident in HBM: row-major [side][side*128] u32 BabyBear (512-byte shares)
+-> row-major [2*side][side*128]. The default workload is the 1024x1024 square
+(512 MiB in, 1 GiB out, both far larger than the 126 MB L2, so no flush is
+needed between steps). Metric: payload Gb/s = side^2 * 512 * 8 / t / 1e9, the
+reference's definition (src/benchmarks/celestia_squares.rs:71-85).
+
+Lines printed by rank 0 (one JSON object):
+  --impl ours       (default) the CUDA library through its C ABI
+  --impl reference  the reference's CPU path (its NTT restated in C,
+                    oracle/zoda_oracle.c) on the host cores, per step a bounded
+                    column sample of the same square
+
+Multi-GPU (torchrun): every rank encodes its own square on its own GPU with
+no collective on the data path (columns are independent); value is the total
+payload of all ranks over the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for sub in ("zoda-cu_b200", "oracle"):
+    sys.path.insert(0, os.path.join(ROOT, sub))
+
+P = 2013265921
+SHARE_U32 = 128
+METRIC = "encode payload Gb/s"
+
+
+def payload_bits(side: int) -> float:
+    return side * side * 512 * 8.0
+
+
+def measured_peaks() -> dict:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def ncu_traffic(kernel_key: str):
+    """Per-launch DRAM bytes of the kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    v = d.get(kernel_key)
+    return None if v is None else float(v.get("dram_bytes_per_launch"))
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (one process per GPU)
+# ---------------------------------------------------------------------------
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's CPU path restated (oracle/zoda_oracle.c)
+# ---------------------------------------------------------------------------
+
+def cpu_port_rate(side: int, budget_s: float, seed: int = 1) -> dict:
+    """Gb/s of the oracle port on a bounded column sample of the side x side square
+    (columns are independent, so a sample of them costs its share of the full square)."""
+    import oracle as O
+    cols = side * SHARE_U32
+    threads = O.num_threads()
+    # calibrate on a small window, then size the sample to the budget
+    probe = max(4, min(cols, 16 * threads))
+    src = O.seeded_input(side, probe, seed=seed)
+    t0 = time.perf_counter()
+    O.encode_rowmajor(src)
+    dt = time.perf_counter() - t0
+    ncols = int(min(cols, max(probe, probe * budget_s / max(dt, 1e-6))))
+    ncols -= ncols % 4
+    src = O.seeded_input(side, ncols, seed=seed)
+    t0 = time.perf_counter()
+    O.encode_rowmajor(src)
+    dt = time.perf_counter() - t0
+    frac = ncols / cols
+    gbps = payload_bits(side) * frac / dt / 1e9
+    return {"value": round(gbps, 4), "unit": "Gb/s", "cores": threads, "kind": "port",
+            "sample": f"{ncols} of {cols} columns of the {side}x{side} square ({100 * frac:.2f}%), "
+                      f"{dt:.2f} s on {threads} threads, oracle/zoda_oracle.c (src/ntt/cpu.rs restated)",
+            "seconds": round(dt, 3)}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    side = args.side
+    rates = []
+    per_step_budget = max(2.0, min(20.0, 60.0 / max(1, args.steps + args.warmup)))
+    for i in range(args.warmup + args.steps):
+        r = cpu_port_rate(side, per_step_budget, seed=1 + i)
+        if i >= args.warmup:
+            rates.append(r)
+    value = statistics.median(r["value"] for r in rates)
+    last = rates[-1]
+    t_step = payload_bits(side) / (value * 1e9) * 1e3
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Gb/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_step, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded uniform in [0,p))",
+        "config": {"workload": f"plain extension of one {side}x{side} square ([{side}][{side * SHARE_U32}] u32 -> "
+                               f"[{2 * side}][{side * SHARE_U32}]), CPU path", "side": side,
+                   "cols": side * SHARE_U32, "l2": "n/a (host)"},
+        "cpu_baseline": {"value": value, "unit": "Gb/s", "cores": last["cores"], "kind": "port",
+                         "sample": last["sample"] + "; ms_per_step extrapolated to the full square"},
+        "e2e": {"value": value, "unit": "Gb/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "gpu_launches": 0,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def time_device_extend(ctx, side: int, steps: int, warmup: int, world: int, sampler=None):
+    """Device-resident extension of one side x side square per step, CUDA events on the launching stream."""
+    import torch
+    cols = side * SHARE_U32
+    gen = torch.Generator(device="cuda").manual_seed(1234 + side)
+    d_in = torch.randint(0, P, (side, cols), dtype=torch.int64, device="cuda", generator=gen).to(torch.int32)
+    d_out = torch.empty((2 * side, cols), dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        ctx.extend(d_in, d_out, side, cols, stream=stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        ctx.extend(d_in, d_out, side, cols, stream=stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = sampler.stop() if sampler else None
+    ms = ev0.elapsed_time(ev1)
+    # spot check of the timed output (even rows are the data)
+    assert torch.equal(d_out[0::2, :256], d_in[:, :256])
+    del d_in, d_out
+    torch.cuda.empty_cache()
+    return ms, clocks
+
+
+def time_host_extend(ctx, side: int, steps: int, warmup: int):
+    """Same extension through the host-buffer C ABI call: H2D + kernel + D2H per step, pinned buffers."""
+    import torch
+    cols = side * SHARE_U32
+    gen = torch.Generator().manual_seed(99)
+    h_in = torch.randint(0, P, (side, cols), dtype=torch.int64, generator=gen).to(torch.int32).pin_memory()
+    h_out = torch.empty((2 * side, cols), dtype=torch.int32).pin_memory()
+    for _ in range(warmup):
+        ctx.extend_host(h_in, h_out, side, cols)
+    tot = 0.0
+    parts = {"h2d_ms": 0.0, "kernel_ms": 0.0, "d2h_ms": 0.0}
+    for _ in range(steps):
+        t = ctx.extend_host(h_in, h_out, side, cols)
+        tot += t.total_ms
+        for k in parts:
+            parts[k] += getattr(t, k)
+    return tot / steps, {k: round(v / steps, 3) for k, v in parts.items()}, side * cols * 4, 2 * side * cols * 4
+
+
+def time_reference_cuda(side: int, iters: int = 2):
+    """The reference's own CUDA kernel (cuda/ntt_kernel.cu built unmodified for sm_100a into
+    oracle/_ref) in its published 'GPU xform' window: intt_cuda(n_k, n_kn) + ntt_cuda(n_kn, n_kn) on a
+    pinned column-major square, PCIe included (src/benchmarks/utils.rs:137-140)."""
+    import ctypes
+    import numpy as np
+    so = os.path.join(ROOT, "oracle", "_ref", "libntt_cuda_ref.so")
+    if not os.path.exists(so):
+        return None
+    ref = ctypes.CDLL(so)
+    ref.cuda_ntt.argtypes = ref.cuda_intt.argtypes = [ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_uint32] * 3
+    ref.cuda_host_alloc.restype = ctypes.c_void_p
+    ref.cuda_host_alloc.argtypes = [ctypes.c_size_t]
+    ref.cuda_host_free.argtypes = [ctypes.c_void_p]
+    import oracle as O
+    cols = side * SHARE_U32
+    n_k, n_kn = side, 2 * side
+    count = n_kn * cols
+    ptr = ref.cuda_host_alloc(count)
+    if not ptr:
+        return None
+    sq = np.frombuffer((ctypes.c_uint32 * count).from_address(ptr), dtype=np.uint32)
+    rk, rkn = O.roots_of_unity(n_k), O.roots_of_unity(n_kn)
+    rng = np.random.default_rng(5)
+    v = sq.reshape(cols, n_kn)
+    v[:, :n_k] = rng.integers(0, P, (cols, n_k), dtype=np.uint32)
+    v[:, n_k:] = 0
+    times = []
+    for i in range(iters + 1):
+        t0 = time.perf_counter()
+        e1 = ref.cuda_intt(ptr, rk.ctypes.data, n_k, cols, n_kn)
+        e2 = ref.cuda_ntt(ptr, rkn.ctypes.data, n_kn, cols, n_kn)
+        dt = time.perf_counter() - t0
+        if e1 or e2:
+            ref.cuda_host_free(ptr)
+            return {"error": f"cuda error {e1} {e2}"}
+        if i:
+            times.append(dt)
+    ref.cuda_host_free(ptr)
+    t = statistics.median(times)
+    return {"side": side, "xform_ms": round(t * 1e3, 2), "gbps": round(payload_bits(side) / t / 1e9, 2),
+            "window": "intt_cuda + ntt_cuda with PCIe (reference's 'GPU xform')"}
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    import zoda_b200
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    ctx = zoda_b200.Context(local)
+    side = args.side
+    cols = side * SHARE_U32
+    sampler = ClockSampler(local) if rank == 0 else None
+    ms, clocks = time_device_extend(ctx, side, args.steps, args.warmup, world, sampler)
+    ms_max = max_over_ranks(ms, world)
+    t_step = ms_max / args.steps
+    value = world * payload_bits(side) / (t_step * 1e-3) / 1e9
+    alg_bytes = 12.0 * side * cols  # read [side][cols] + write [2 side][cols] u32
+    peaks = measured_peaks()
+    achieved = alg_bytes / (ms / args.steps * 1e-3) / 1e9
+    traffic = ncu_traffic(f"k_extend_side{side}")
+    extra = {}
+    e2e = None
+    cpu = None
+    if rank == 0:
+        e2e_ms, parts, h2d, d2h = time_host_extend(ctx, side, max(2, min(args.steps, 5)), 1)
+        e2e = {"value": round(payload_bits(side) / (e2e_ms * 1e-3) / 1e9, 3), "unit": "Gb/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_ms, 3),
+               "split_ms": parts, "api": "zoda_extend_host (pinned host buffers)"}
+    if world > 1:
+        barrier(world)
+    if rank == 0 and not args.no_extra:
+        for s2 in args.extra_sides:
+            if s2 == side:
+                continue
+            ms2, _ = time_device_extend(ctx, s2, max(3, args.steps // 2), 3, 1)
+            t2 = ms2 / max(3, args.steps // 2)
+            extra[f"side{s2}"] = {
+                "ms_per_step": round(t2, 4), "gbps": round(payload_bits(s2) / (t2 * 1e-3) / 1e9, 1),
+                "hbm_frac": round(12.0 * s2 * s2 * SHARE_U32 / (t2 * 1e-3) / 1e9 / peaks["hbm_gbs"], 4)}
+        refc = time_reference_cuda(min(side, 1024))
+        if refc:
+            extra["reference_cuda_kernel"] = refc
+    if rank == 0:
+        cpu = cpu_port_rate(side, args.cpu_budget)
+        cpu.pop("seconds", None)
+    if world > 1:
+        barrier(world)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "Gb/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(t_step, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded uniform in [0,p), device-resident)",
+            "config": {"workload": f"plain device-resident extension of one {side}x{side} square per GPU "
+                                   f"([{side}][{cols}] u32 -> [{2 * side}][{cols}])",
+                       "side": side, "cols": cols, "share_bytes": 512,
+                       "l2": "inputs (and outputs) larger than the 126 MB L2; no flush"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
+                         "peak_source": peaks["source"], "kernel": f"k_extend<{side.bit_length() - 1}>",
+                         "alg_bytes_per_launch": alg_bytes},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": args.steps,
+            "clocks": clocks,
+            "extra": extra,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--side", type=int, default=1024)
+    ap.add_argument("--extra-sides", type=int, nargs="*", default=[2048, 4096])
+    ap.add_argument("--no-extra", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=10.0, help="seconds of CPU baseline sampling")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

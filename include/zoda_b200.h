@@ -1,0 +1,121 @@
+/*
+ * zoda_b200.h -- C ABI of libzoda_b200.so, the sm_100a replacement for
+ * zoda-cu's column-wise Reed-Solomon extension over BabyBear
+ * (p = 2^31 - 2^27 + 1).
+ *
+ * Part 1 is the reference's own FFI, symbol for symbol: a Rust crate that
+ * declares the block in src/ntt/cuda.rs:15-22 links against this library
+ * unchanged (as libntt_cuda.a or this .so).
+ *
+ * Part 2 adds device-resident calls behind a context: the fused extension
+ * (one HBM pass, row-major in and out), its host-buffer variant, the batched
+ * multi-square launch and the serving loop.
+ *
+ * All element buffers hold canonical u32 BabyBear values in [0, p).
+ * No call aborts the process; every failure comes back as a status code.
+ */
+#ifndef ZODA_B200_H
+#define ZODA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ======================================================================
+ * Part 1: the reference FFI (cuda/ntt_kernel.cu:184-208)
+ * ====================================================================== */
+
+/* Replaces cuda/ntt_kernel.cu:190-193 (bound at src/ntt/cuda.rs:17).
+ * Forward NTT, in place, of `polys` polynomials laid `stride` u32 apart in
+ * host memory (pinned from cuda_host_alloc is fastest, pageable works).
+ * Only values[c*stride .. c*stride + n) are transformed; the rest of each
+ * polynomial is left untouched. roots = [w^0 .. w^(n-1)] for a primitive
+ * n-th root w (src/ntt/cuda.rs:111-114 passes roots_of_unity(n)). Natural
+ * order in and out. Returns 0 on success, else a nonzero cudaError_t value
+ * (cudaErrorInvalidValue = 1 for bad arguments, including a roots table
+ * that is not the powers of a primitive n-th root). Synchronous. */
+int cuda_ntt(uint32_t* values, const uint32_t* roots, uint32_t n, uint32_t polys, uint32_t stride);
+
+/* Replaces cuda/ntt_kernel.cu:196-208 (bound at src/ntt/cuda.rs:18).
+ * Inverse NTT with the same layout: the transform with inverse roots
+ * [roots[0], roots[n-1], ..., roots[1]], then every value times n^-1. */
+int cuda_intt(uint32_t* values, const uint32_t* roots, uint32_t n, uint32_t polys, uint32_t stride);
+
+/* Replaces cuda/ntt_kernel.cu:184-187 (bound at src/ntt/cuda.rs:19):
+ * pinned host allocation of `count` u32, NULL on failure. */
+uint32_t* cuda_host_alloc(size_t count);
+
+/* Replaces cuda/ntt_kernel.cu:188 (bound at src/ntt/cuda.rs:20). */
+void cuda_host_free(uint32_t* p);
+
+/* src/ntt/cuda.rs:21 also binds cudaGetDeviceCount; it resolves from the
+ * CUDA runtime this library links. */
+
+/* ======================================================================
+ * Part 2: device-resident API
+ * ====================================================================== */
+
+typedef enum zoda_status {
+    ZODA_OK = 0,
+    ZODA_ERR_ARG = 1,         /* bad argument (size, alignment, null)        */
+    ZODA_ERR_CUDA = 2,        /* a CUDA call failed; see zoda_last_error     */
+    ZODA_ERR_NOMEM = 3,       /* device or host allocation failed            */
+    ZODA_ERR_UNSUPPORTED = 4, /* shape this build does not handle            */
+    ZODA_ERR_BUDGET = 5,      /* request exceeds the admission budget        */
+    ZODA_ERR_TIMEOUT = 6,     /* a bounded wait ran out                      */
+    ZODA_ERR_CANCELLED = 7,   /* request cancelled before it ran             */
+    ZODA_ERR_STATE = 8        /* call not valid in the object's state        */
+} zoda_status;
+
+typedef struct zoda_ctx zoda_ctx;
+
+/* Human-readable name of a status. */
+const char* zoda_status_string(zoda_status s);
+/* Text of the last CUDA error seen on this thread ("" if none). */
+const char* zoda_last_error(void);
+
+/* Creates a context on `device`: uploads the twiddle tables (omega_8192^j
+ * and, per side S, g^i / S with g = omega_2S) and sets kernel attributes.
+ * Replaces the per-call root generation and upload of src/ntt/cuda.rs:112
+ * and cuda/ntt_kernel.cu:111-114. */
+zoda_status zoda_ctx_create(int device, zoda_ctx** out);
+void zoda_ctx_destroy(zoda_ctx* ctx);
+
+/* Largest k the fused extension accepts (4096). */
+uint32_t zoda_max_side(void);
+
+/* Fused extension, device memory. d_in is row-major [k][cols], d_out is
+ * row-major [2k][cols]; row j of d_out is every column's degree-<k
+ * interpolant evaluated at omega_2k^j, i.e. the rows the reference gathers
+ * from its column-major square (src/benchmarks/utils.rs:167-168,
+ * src/zoda/babybear.rs:155): even rows equal the input rows. k must be a
+ * power of two in [1, zoda_max_side()], cols a multiple of 4, both pointers
+ * 16-byte aligned and non-overlapping. Asynchronous on `stream`, a
+ * cudaStream_t (NULL is the legacy default stream, as in every CUDA API). */
+zoda_status zoda_extend_device(zoda_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t k, uint64_t cols,
+                               void* stream);
+
+/* Timing of a host-buffer call, in milliseconds (CUDA events). */
+typedef struct zoda_timing {
+    float h2d_ms;    /* host -> device copy of the input        */
+    float kernel_ms; /* the fused extension kernel              */
+    float d2h_ms;    /* device -> host copy of the output       */
+    float total_ms;  /* first copy start to last copy end       */
+} zoda_timing;
+
+/* Fused extension from host memory to host memory: the reference's
+ * `encode_gpu` window (src/benchmarks/utils.rs:100-146) without the host
+ * transpose and padding, which the kernel makes unnecessary. h_in row-major
+ * [k][cols], h_out row-major [2k][cols]; pinned buffers give full PCIe speed.
+ * Device buffers are taken from the context's cache. Synchronous.
+ * `timing` may be NULL. */
+zoda_status zoda_extend_host(zoda_ctx* ctx, const uint32_t* h_in, uint32_t* h_out, uint32_t k, uint64_t cols,
+                             zoda_timing* timing);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ZODA_B200_H */

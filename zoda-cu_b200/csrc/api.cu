@@ -1,0 +1,217 @@
+// Context, twiddle tables, status reporting and the fused-extension entry
+// points of the C ABI (include/zoda_b200.h, part 2).
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "internal.hpp"
+
+namespace zb {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_last_error(const char* where, cudaError_t e) {
+    char buf[512];
+    snprintf(buf, sizeof buf, "%s: %s (%d)", where, cudaGetErrorString(e), (int)e);
+    g_last_error = buf;
+}
+void set_last_error_text(const std::string& s) { g_last_error = s; }
+
+zoda_status DevBuf::ensure(size_t need) {
+    if (need <= bytes) return ZODA_OK;
+    release();
+    if (need == 0) return ZODA_OK;
+    cudaError_t e = cudaMalloc(&p, need);
+    if (e != cudaSuccess) {
+        set_last_error("cudaMalloc", e);
+        p = nullptr;
+        return ZODA_ERR_NOMEM;
+    }
+    bytes = need;
+    return ZODA_OK;
+}
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+static uint32_t powmod(uint32_t b, uint64_t e) { return powmod_c(b, e); }
+
+// Host-built tables: tw[j] = omega_8192^j; twist[S + i] = omega_2S^i / S.
+static void build_tables(std::vector<Tw>& tw, std::vector<Tw>& twist) {
+    constexpr int LOG_TW = 13;
+    const uint32_t n = 1u << LOG_TW;
+    tw.resize(n);
+    const uint32_t w = root_of_unity(LOG_TW);
+    uint32_t cur = 1;
+    for (uint32_t j = 0; j < n; j++) {
+        tw[j] = Tw{cur, shoup(cur)};
+        cur = mulmod_c(cur, w);
+    }
+    twist.assign(n, Tw{0, 0});
+    for (int ls = 0; ls <= 12; ls++) {
+        const uint32_t S = 1u << ls;
+        const uint32_t g = root_of_unity(ls + 1);
+        const uint32_t s_inv = powmod(S, P - 2);
+        uint32_t c = s_inv;
+        for (uint32_t i = 0; i < S; i++) {
+            twist[S + i] = Tw{c, shoup(c)};
+            c = mulmod_c(c, g);
+        }
+    }
+}
+
+static int log2_exact(uint64_t x) {
+    if (x == 0 || (x & (x - 1))) return -1;
+    int l = 0;
+    while ((1ull << l) < x) l++;
+    return l;
+}
+
+}  // namespace zb
+
+using namespace zb;
+
+extern "C" {
+
+const char* zoda_status_string(zoda_status s) {
+    switch (s) {
+        case ZODA_OK: return "ok";
+        case ZODA_ERR_ARG: return "invalid argument";
+        case ZODA_ERR_CUDA: return "CUDA error";
+        case ZODA_ERR_NOMEM: return "out of memory";
+        case ZODA_ERR_UNSUPPORTED: return "unsupported shape";
+        case ZODA_ERR_BUDGET: return "over the admission budget";
+        case ZODA_ERR_TIMEOUT: return "timed out";
+        case ZODA_ERR_CANCELLED: return "cancelled";
+        case ZODA_ERR_STATE: return "invalid state";
+    }
+    return "unknown status";
+}
+
+const char* zoda_last_error(void) { return g_last_error.c_str(); }
+
+uint32_t zoda_max_side(void) { return 4096u; }
+
+zoda_status zoda_ctx_create(int device, zoda_ctx** out) {
+    if (!out) return ZODA_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    ZB_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return ZODA_ERR_ARG;
+    ZB_CUDA(cudaSetDevice(device));
+    zoda_ctx* c = new (std::nothrow) zoda_ctx();
+    if (!c) return ZODA_ERR_NOMEM;
+    c->device = device;
+    auto fail = [&](zoda_status s) {
+        zoda_ctx_destroy(c);
+        return s;
+    };
+    cudaError_t e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) {
+        set_last_error("cudaDeviceGetAttribute", e);
+        return fail(ZODA_ERR_CUDA);
+    }
+    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+        set_last_error("cudaStreamCreate", e);
+        return fail(ZODA_ERR_CUDA);
+    }
+    for (auto& ev : c->ev) {
+        if ((e = cudaEventCreate(&ev)) != cudaSuccess) {
+            set_last_error("cudaEventCreate", e);
+            return fail(ZODA_ERR_CUDA);
+        }
+    }
+    std::vector<Tw> tw, twist;
+    build_tables(tw, twist);
+    if ((e = cudaMalloc(&c->tables.tw, tw.size() * sizeof(Tw))) != cudaSuccess ||
+        (e = cudaMalloc(&c->tables.twist, twist.size() * sizeof(Tw))) != cudaSuccess) {
+        set_last_error("cudaMalloc(tables)", e);
+        return fail(ZODA_ERR_NOMEM);
+    }
+    if ((e = cudaMemcpy(c->tables.tw, tw.data(), tw.size() * sizeof(Tw), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(c->tables.twist, twist.data(), twist.size() * sizeof(Tw), cudaMemcpyHostToDevice)) !=
+            cudaSuccess) {
+        set_last_error("cudaMemcpy(tables)", e);
+        return fail(ZODA_ERR_CUDA);
+    }
+    zoda_status s = extend_init_attributes();
+    if (s != ZODA_OK) return fail(s);
+    *out = c;
+    return ZODA_OK;
+}
+
+void zoda_ctx_destroy(zoda_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    c->in_buf.release();
+    c->out_buf.release();
+    if (c->tables.tw) cudaFree(c->tables.tw);
+    if (c->tables.twist) cudaFree(c->tables.twist);
+    for (auto& ev : c->ev)
+        if (ev) cudaEventDestroy(ev);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+static zoda_status check_extend_args(const zoda_ctx* ctx, const void* in, const void* out, uint32_t k, uint64_t cols,
+                                     int* log_s) {
+    if (!ctx || !in || !out) return ZODA_ERR_ARG;
+    const int ls = log2_exact(k);
+    if (ls < 0) return ZODA_ERR_ARG;
+    if (k > zoda_max_side()) return ZODA_ERR_UNSUPPORTED;
+    if (cols % 4 != 0) return ZODA_ERR_ARG;
+    if (((uintptr_t)in | (uintptr_t)out) & 15) return ZODA_ERR_ARG;
+    *log_s = ls;
+    return ZODA_OK;
+}
+
+zoda_status zoda_extend_device(zoda_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t k, uint64_t cols,
+                               void* stream) {
+    int ls = 0;
+    zoda_status s = check_extend_args(ctx, d_in, d_out, k, cols, &ls);
+    if (s != ZODA_OK) return s;
+    const uint64_t in_bytes = (uint64_t)k * cols * 4;
+    const char* a = (const char*)d_in;
+    const char* b = (const char*)d_out;
+    if (a < b + 2 * in_bytes && b < a + in_bytes) return ZODA_ERR_ARG;  // overlap
+    if (cols == 0) return ZODA_OK;
+    ZB_CUDA(cudaSetDevice(ctx->device));
+    return launch_extend(ctx, ls, d_in, d_out, cols, (cudaStream_t)stream);
+}
+
+zoda_status zoda_extend_host(zoda_ctx* ctx, const uint32_t* h_in, uint32_t* h_out, uint32_t k, uint64_t cols,
+                             zoda_timing* timing) {
+    int ls = 0;
+    zoda_status s = check_extend_args(ctx, h_in, h_out, k, cols, &ls);
+    if (s != ZODA_OK) return s;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ZB_CUDA(cudaSetDevice(ctx->device));
+    const size_t in_bytes = (size_t)k * cols * 4, out_bytes = 2 * in_bytes;
+    if ((s = ctx->in_buf.ensure(in_bytes)) != ZODA_OK) return s;
+    if ((s = ctx->out_buf.ensure(out_bytes)) != ZODA_OK) return s;
+    cudaStream_t st = ctx->stream;
+    ZB_CUDA(cudaEventRecord(ctx->ev[0], st));
+    ZB_CUDA(cudaMemcpyAsync(ctx->in_buf.p, h_in, in_bytes, cudaMemcpyHostToDevice, st));
+    ZB_CUDA(cudaEventRecord(ctx->ev[1], st));
+    if ((s = launch_extend(ctx, ls, (const uint32_t*)ctx->in_buf.p, (uint32_t*)ctx->out_buf.p, cols, st)) != ZODA_OK)
+        return s;
+    ZB_CUDA(cudaEventRecord(ctx->ev[2], st));
+    ZB_CUDA(cudaMemcpyAsync(h_out, ctx->out_buf.p, out_bytes, cudaMemcpyDeviceToHost, st));
+    ZB_CUDA(cudaEventRecord(ctx->ev[3], st));
+    ZB_CUDA(cudaEventSynchronize(ctx->ev[3]));
+    if (timing) {
+        ZB_CUDA(cudaEventElapsedTime(&timing->h2d_ms, ctx->ev[0], ctx->ev[1]));
+        ZB_CUDA(cudaEventElapsedTime(&timing->kernel_ms, ctx->ev[1], ctx->ev[2]));
+        ZB_CUDA(cudaEventElapsedTime(&timing->d2h_ms, ctx->ev[2], ctx->ev[3]));
+        ZB_CUDA(cudaEventElapsedTime(&timing->total_ms, ctx->ev[0], ctx->ev[3]));
+    }
+    return ZODA_OK;
+}
+
+}  // extern "C"

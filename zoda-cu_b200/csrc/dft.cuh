@@ -1,0 +1,93 @@
+// Register-resident DFT building blocks shared by every kernel in the library.
+//
+// A thread holds a small group of field elements per column in registers,
+// always for four adjacent columns at once (a "quad", one 16-byte vector), so
+// every twiddle it loads or computes is reused four times.
+//
+// dft_dif<LOG_R, INV> runs the radix-2^LOG_R Gentleman-Sande network on the
+// register group: natural-order input, bit-reversed output (register r holds
+// output index bitrev(r)). Its internal twiddles are compile-time constants,
+// so they become immediate operands.
+#pragma once
+#include <cstdint>
+#include <utility>
+
+#include "field.cuh"
+
+namespace zb {
+
+struct V4 {
+    uint32_t c[4];
+};
+
+__device__ __forceinline__ V4 ld_v4(const uint32_t* p) {
+    uint4 u = *reinterpret_cast<const uint4*>(p);
+    return V4{{u.x, u.y, u.z, u.w}};
+}
+__device__ __forceinline__ void st_v4(uint32_t* p, const V4& v) {
+    *reinterpret_cast<uint4*>(p) = make_uint4(v.c[0], v.c[1], v.c[2], v.c[3]);
+}
+// streaming (evict-first) variants for data touched once
+__device__ __forceinline__ V4 ldg_stream_v4(const uint32_t* p) {
+    uint4 u = __ldcs(reinterpret_cast<const uint4*>(p));
+    return V4{{u.x, u.y, u.z, u.w}};
+}
+__device__ __forceinline__ void stg_stream_v4(uint32_t* p, const V4& v) {
+    __stcs(reinterpret_cast<uint4*>(p), make_uint4(v.c[0], v.c[1], v.c[2], v.c[3]));
+}
+
+__host__ __device__ constexpr int bitrev(int x, int bits) {
+    int r = 0;
+    for (int i = 0; i < bits; i++) r |= ((x >> i) & 1) << (bits - 1 - i);
+    return r;
+}
+
+__device__ __forceinline__ void bfly4(V4& a, V4& b, uint32_t w, uint32_t ws) {
+#pragma unroll
+    for (int c = 0; c < 4; c++) dif_bfly(a.c[c], b.c[c], w, ws);
+}
+__device__ __forceinline__ void bfly4_1(V4& a, V4& b) {
+#pragma unroll
+    for (int c = 0; c < 4; c++) dif_bfly1(a.c[c], b.c[c]);
+}
+__device__ __forceinline__ void mul4(V4& a, const Tw t) {
+#pragma unroll
+    for (int c = 0; c < 4; c++) a.c[c] = mul_tw(a.c[c], t.w, t.ws);
+}
+
+namespace detail {
+template <bool INV, int LH, int J>
+__device__ __forceinline__ void bfly_at(V4* x) {
+    constexpr int h = 1 << LH;
+    if constexpr ((J & h) == 0) {
+        constexpr int e = J & (h - 1);
+        if constexpr (e == 0) {
+            bfly4_1(x[J], x[J + h]);
+        } else {
+            constexpr uint32_t w = root_pow(LH + 1, (uint32_t)e, INV);
+            constexpr uint32_t ws = shoup(w);
+            bfly4(x[J], x[J + h], w, ws);
+        }
+    }
+}
+template <bool INV, int LH, int... Js>
+__device__ __forceinline__ void stage(V4* x, std::integer_sequence<int, Js...>) {
+    (bfly_at<INV, LH, Js>(x), ...);
+}
+template <bool INV, int LOG_R, int LH>
+__device__ __forceinline__ void stages(V4* x) {
+    if constexpr (LH >= 0) {
+        stage<INV, LH>(x, std::make_integer_sequence<int, (1 << LOG_R)>{});
+        stages<INV, LOG_R, LH - 1>(x);
+    }
+}
+}  // namespace detail
+
+// In-register DIF DFT of size 2^LOG_R over x[0..2^LOG_R), four columns at once.
+// INV selects omega^-1 (the transform src/ntt/cpu.rs:48-60 runs before its n^-1 scale).
+template <int LOG_R, bool INV>
+__device__ __forceinline__ void dft_dif(V4* x) {
+    detail::stages<INV, LOG_R, LOG_R - 1>(x);
+}
+
+}  // namespace zb

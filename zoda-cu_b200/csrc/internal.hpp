@@ -1,0 +1,62 @@
+// Library-internal declarations shared by the .cu translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+
+#include "../../include/zoda_b200.h"
+#include "field.cuh"
+
+namespace zb {
+
+// Per-thread record of the last CUDA failure, returned by zoda_last_error().
+void set_last_error(const char* where, cudaError_t e);
+void set_last_error_text(const std::string& s);
+
+#define ZB_CUDA(call)                                \
+    do {                                             \
+        cudaError_t zb_e_ = (call);                  \
+        if (zb_e_ != cudaSuccess) {                  \
+            ::zb::set_last_error(#call, zb_e_);      \
+            return ZODA_ERR_CUDA;                    \
+        }                                            \
+    } while (0)
+
+// Grow-only device buffer owned by a context.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    zoda_status ensure(size_t need);
+    void release();
+};
+
+// Twiddle tables in HBM, built once per context:
+//   tw[j]            = omega_8192^j with its Shoup companion, j in [0, 8192)
+//   twist[S + i]     = omega_2S^i * S^-1, i in [0, S), for S = 1 .. 4096
+struct Tables {
+    Tw* tw = nullptr;
+    Tw* twist = nullptr;
+};
+
+}  // namespace zb
+
+struct zoda_ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    zb::Tables tables;
+    // host-call staging
+    zb::DevBuf in_buf, out_buf;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    std::mutex mu;  // serialises host calls on one context
+};
+
+namespace zb {
+// Launches the fused extension kernel for side 2^log_s (0 <= log_s <= 12).
+zoda_status launch_extend(const zoda_ctx* ctx, int log_s, const uint32_t* in, uint32_t* out, uint64_t cols,
+                          cudaStream_t st);
+// Sets the dynamic shared memory attribute of every extension instantiation.
+zoda_status extend_init_attributes();
+}  // namespace zb

@@ -1,0 +1,247 @@
+"""Python host binding of libzoda_b200.so (the C ABI in include/zoda_b200.h).
+
+This is the host-side mirror of the reference's encode API for this path:
+  * ``ntt_cuda`` / ``intt_cuda`` keep the argument meaning and the error
+    behaviour of src/ntt/cuda.rs:99-131 (power-of-two n, stride >= n, whole
+    polynomials; a CUDA failure raises with the error code);
+  * ``PinnedSquare`` mirrors src/ntt/cuda.rs:34-97 (column-major pinned u32);
+  * ``Context.extend`` is the fused device-resident extension that replaces
+    ``encode_gpu`` (src/benchmarks/utils.rs:100-146) and ``extend``
+    (src/zoda/babybear.rs:34-46) for k = n = side.
+
+The library must be built (``make -C zoda-cu_b200``); there is no fallback:
+every call here runs the CUDA kernels or raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libzoda_b200.so")
+
+P = 2013265921
+ZODA_OK = 0
+STATUS = {
+    0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory", 4: "unsupported shape",
+    5: "over the admission budget", 6: "timed out", 7: "cancelled", 8: "invalid state",
+}
+
+# every symbol include/zoda_b200.h declares
+EXPORTS = [
+    "cuda_ntt", "cuda_intt", "cuda_host_alloc", "cuda_host_free",
+    "zoda_status_string", "zoda_last_error", "zoda_ctx_create", "zoda_ctx_destroy", "zoda_max_side",
+    "zoda_extend_device", "zoda_extend_host",
+]
+
+_lib = None
+
+
+class ZodaError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str = ""):
+        self.status = status
+        super().__init__(f"{where}: {STATUS.get(status, status)}" + (f" ({detail})" if detail else ""))
+
+
+class ZodaTiming(ctypes.Structure):
+    _fields_ = [("h2d_ms", ctypes.c_float), ("kernel_ms", ctypes.c_float),
+                ("d2h_ms", ctypes.c_float), ("total_ms", ctypes.c_float)]
+
+
+def load(path: str = LIB_PATH):
+    """Load the library and declare every exported signature. Raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is not built; run `make -C {HERE}`")
+    L = ctypes.CDLL(path)
+    u32p = ctypes.POINTER(ctypes.c_uint32)
+    vp = ctypes.c_void_p
+    L.cuda_ntt.restype = ctypes.c_int
+    L.cuda_ntt.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
+    L.cuda_intt.restype = ctypes.c_int
+    L.cuda_intt.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
+    L.cuda_host_alloc.restype = vp
+    L.cuda_host_alloc.argtypes = [ctypes.c_size_t]
+    L.cuda_host_free.restype = None
+    L.cuda_host_free.argtypes = [vp]
+    L.zoda_status_string.restype = ctypes.c_char_p
+    L.zoda_status_string.argtypes = [ctypes.c_int]
+    L.zoda_last_error.restype = ctypes.c_char_p
+    L.zoda_last_error.argtypes = []
+    L.zoda_ctx_create.restype = ctypes.c_int
+    L.zoda_ctx_create.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
+    L.zoda_ctx_destroy.restype = None
+    L.zoda_ctx_destroy.argtypes = [vp]
+    L.zoda_max_side.restype = ctypes.c_uint32
+    L.zoda_max_side.argtypes = []
+    L.zoda_extend_device.restype = ctypes.c_int
+    L.zoda_extend_device.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.c_uint64, vp]
+    L.zoda_extend_host.restype = ctypes.c_int
+    L.zoda_extend_host.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(ZodaTiming)]
+    del u32p
+    _lib = L
+    return L
+
+
+def _check(status: int, where: str):
+    if status != ZODA_OK:
+        detail = load().zoda_last_error().decode(errors="replace")
+        raise ZodaError(status, where, detail)
+
+
+def _addr(buf) -> int:
+    """Address of a torch tensor, numpy array or raw int pointer."""
+    if isinstance(buf, int):
+        return buf
+    if hasattr(buf, "data_ptr"):
+        return buf.data_ptr()
+    if hasattr(buf, "ctypes"):
+        return buf.ctypes.data
+    raise TypeError(f"cannot take the address of {type(buf)}")
+
+
+class Context:
+    """A device context: twiddle tables resident in HBM, a stream, cached buffers."""
+
+    def __init__(self, device: int = 0):
+        L = load()
+        h = ctypes.c_void_p()
+        _check(L.zoda_ctx_create(device, ctypes.byref(h)), "zoda_ctx_create")
+        self._h = h
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            load().zoda_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def extend(self, d_in, d_out, k: int, cols: int, stream=None):
+        """Fused extension on device buffers: d_in [k][cols] -> d_out [2k][cols] (row-major u32).
+        `stream` is a torch.cuda.Stream, a raw cudaStream_t int, or None for torch's current
+        stream (so torch events and later torch work order correctly against the kernel)."""
+        if stream is None:
+            import torch
+            stream = torch.cuda.current_stream()
+        s = stream if isinstance(stream, int) else stream.cuda_stream
+        _check(load().zoda_extend_device(self._h, _addr(d_in), _addr(d_out), k, cols, s or None),
+               "zoda_extend_device")
+
+    def extend_host(self, h_in, h_out, k: int, cols: int) -> ZodaTiming:
+        t = ZodaTiming()
+        _check(load().zoda_extend_host(self._h, _addr(h_in), _addr(h_out), k, cols, ctypes.byref(t)),
+               "zoda_extend_host")
+        return t
+
+
+def max_side() -> int:
+    return int(load().zoda_max_side())
+
+
+# ---- mirror of src/ntt/cuda.rs ----------------------------------------------
+
+def cuda_available() -> bool:
+    """src/ntt/cuda.rs:25-29 through the CUDA runtime the library links."""
+    try:
+        import torch
+        return torch.cuda.is_available() and torch.cuda.device_count() > 0
+    except Exception:
+        return False
+
+
+def _run(values, n: int, stride: int, fn, name: str, roots=None):
+    """src/ntt/cuda.rs:99-119: argument checks, roots_of_unity(n), the FFI call."""
+    import numpy as np
+    assert n > 0 and (n & (n - 1)) == 0, "NTT size must be power of 2"
+    assert stride >= n, "stride must be at least n"
+    size = values.size if hasattr(values, "size") and not callable(values.size) else values.numel()
+    assert stride > 0 and size % stride == 0, "values must be whole polynomials of stride elements"
+    polys = size // stride
+    if roots is None:
+        roots = _roots_of_unity(n)
+    roots = np.ascontiguousarray(roots, dtype=np.uint32)
+    err = fn(_addr(values), roots.ctypes.data, n, polys, stride)
+    if err != 0:
+        raise RuntimeError(f"{name} failed with CUDA error {err}")
+
+
+def _roots_of_unity(n: int):
+    """[w^0 .. w^(n-1)] for w = 31^((p-1)/n), the roots src/ntt/cpu.rs:96-110 derives."""
+    import numpy as np
+    w = pow(31, (P - 1) // n, P)
+    out = np.empty(n, dtype=np.uint32)
+    cur = 1
+    for i in range(n):
+        out[i] = cur
+        cur = cur * w % P
+    return out
+
+
+def ntt_cuda(values, n: int, stride: int, roots=None):
+    """src/ntt/cuda.rs:124-126: forward NTT on the GPU, in place, host buffer."""
+    _run(values, n, stride, load().cuda_ntt, "cuda_ntt", roots)
+
+
+def intt_cuda(values, n: int, stride: int, roots=None):
+    """src/ntt/cuda.rs:129-131: inverse NTT on the GPU, in place, host buffer."""
+    _run(values, n, stride, load().cuda_intt, "cuda_intt", roots)
+
+
+class PinnedSquare:
+    """src/ntt/cuda.rs:34-97: `cols` polynomials of `rows` canonical u32 each, column-major,
+    in pinned host memory from cuda_host_alloc; element (row, col) at col*rows + row."""
+
+    def __init__(self, rows: int, cols: int):
+        import numpy as np
+        count = max(rows * cols, 1)
+        ptr = load().cuda_host_alloc(count)
+        if not ptr:
+            raise MemoryError(f"cudaHostAlloc of {count} u32 failed")
+        self._ptr = ptr
+        self.rows, self.cols = rows, cols
+        buf = (ctypes.c_uint32 * count).from_address(ptr)
+        self.array = np.frombuffer(buf, dtype=np.uint32, count=rows * cols)
+        self.array[:] = 0
+
+    def set(self, row, col, value):
+        self.array[col * self.rows + row] = value
+
+    def get(self, row, col):
+        return int(self.array[col * self.rows + row])
+
+    def column(self, col):
+        return self.array[col * self.rows:(col + 1) * self.rows]
+
+    def row(self, row):
+        return self.array[row::self.rows][:self.cols]
+
+    @property
+    def size(self):
+        return self.rows * self.cols
+
+    @property
+    def ctypes(self):
+        return self.array.ctypes
+
+    def free(self):
+        if self._ptr:
+            self.array = None
+            load().cuda_host_free(self._ptr)
+            self._ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
