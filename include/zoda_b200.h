@@ -87,6 +87,22 @@ void zoda_ctx_destroy(zoda_ctx* ctx);
 /* Largest k the fused extension accepts (4096). */
 uint32_t zoda_max_side(void);
 
+/* Kernel variant of the fused extension on a context. AUTO picks the
+ * TMA-staged kernel for 128 <= k <= 2048 and the direct-load kernel
+ * otherwise; the others force one (for tests and tuning; TMA supports k in
+ * [128, 4096]). */
+typedef enum zoda_extend_impl {
+    ZODA_IMPL_AUTO = 0,
+    ZODA_IMPL_DIRECT = 1,
+    ZODA_IMPL_TMA = 2
+} zoda_extend_impl;
+zoda_status zoda_ctx_set_impl(zoda_ctx* ctx, int impl);
+
+/* Returns ZODA_ERR_TIMEOUT (and clears the flag) if a kernel on this context
+ * gave up a bounded wait since the last call, else ZODA_OK. Synchronizes the
+ * device first. */
+zoda_status zoda_ctx_check(zoda_ctx* ctx);
+
 /* Fused extension, device memory. d_in is row-major [k][cols], d_out is
  * row-major [2k][cols]; row j of d_out is every column's degree-<k
  * interpolant evaluated at omega_2k^j, i.e. the rows the reference gathers

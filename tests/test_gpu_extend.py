@@ -45,14 +45,35 @@ def tile_cols(side: int) -> int:
     return 2048 if side <= 16 else 32768 // side
 
 
-@pytest.mark.parametrize("side", [1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096])
-def test_extend_matches_oracle_all_sides(ctx, side):
-    # two full tiles plus a ragged third (still a multiple of 4 columns)
+SIDES = [1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096]
+IMPLS = [(s, 1) for s in SIDES] + [(s, 2) for s in SIDES if s >= 128]
+
+
+@pytest.mark.parametrize("side,impl", IMPLS, ids=[f"side{s}-{'direct' if i == 1 else 'tma'}" for s, i in IMPLS])
+def test_extend_matches_oracle_all_sides(ctx, side, impl):
+    # both kernel variants; two full tiles plus a ragged third (still a multiple of 4 columns)
     cols = 2 * tile_cols(side) + 12 if side > 1 else 36
     data = O.seeded_input(side, cols, seed=100 + side)
-    got = run_extend(ctx, data)
+    ctx.set_impl(impl)
+    try:
+        got = run_extend(ctx, data)
+        ctx.check()
+    finally:
+        ctx.set_impl(0)
     want = O.encode_rowmajor(data)
     assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("side", [128, 1024, 2048])
+def test_extend_many_tiles_per_cta(ctx, side):
+    # more tiles than SMs, so every CTA loops and reuses its staging buffer
+    cols = 148 * 3 * tile_cols(side) + 40
+    data = O.seeded_input(side, cols, seed=300 + side)
+    got = run_extend(ctx, data)
+    ctx.check()
+    idx = np.r_[0:64, cols // 2:cols // 2 + 64, cols - 64:cols]
+    want = O.encode_rowmajor(data[:, idx])
+    assert np.array_equal(got[:, idx], want)
 
 
 def test_extend_config_side64_full(ctx):

@@ -65,6 +65,62 @@ static void build_tables(std::vector<Tw>& tw, std::vector<Tw>& twist) {
     }
 }
 
+// Level tables of the TMA-staged kernel for side 2^ls (layout documented at
+// SideTables in extend_tma.cuh). Offsets are entries into `all`.
+static void build_side_tables(int ls, std::vector<Tw>& all, size_t off[5]) {
+    const int nlev = (ls + 3) / 4;
+    auto lr = [&](int l) { return l < nlev - 1 ? 4 : ls - 4 * (nlev - 1); };
+    auto nlr = [&](int l) { return lr(nlev - 1 - l); };
+    const uint32_t S = 1u << ls;
+    auto tw_of = [](uint32_t w) { return Tw{w, shoup(w)}; };
+    auto pow_root = [](int logn, uint64_t e) { return powmod_c(root_of_unity(logn), e); };
+    for (int k = 0; k < 5; k++) off[k] = all.size();
+    // INTT levels 0 .. nlev-2: [k2*L + m] = omega_N^(-m*k2)
+    int pb = 0;
+    for (int l = 0; l < 2; l++) {
+        off[l] = all.size();
+        if (l < nlev - 1) {
+            const int logn = ls - pb, R = 1 << lr(l), L = 1 << (logn - lr(l));
+            const uint32_t N = 1u << logn;
+            for (int k2 = 0; k2 < R; k2++)
+                for (int m = 0; m < L; m++) all.push_back(tw_of(pow_root(logn, (N - (uint64_t)m * k2 % N) % N)));
+            pb += lr(l);
+        }
+    }
+    // NTT level 0 with the twist: [k2*NB + b] = g^c0 / S * omega_S^(c0*k2)
+    off[2] = all.size();
+    {
+        const int LR = lr(nlev - 1), R = 1 << LR;
+        const uint32_t NB = S >> LR;
+        const uint32_t g = root_of_unity(ls + 1);
+        const uint32_t s_inv = powmod_c(S, P - 2);
+        for (int k2 = 0; k2 < R; k2++)
+            for (uint32_t b = 0; b < NB; b++) {
+                // c0 = digit reversal of slot b*R over the INTT radices
+                uint32_t slot = b << LR, c0 = 0;
+                int sh_in = ls, sh_out = 0;
+                for (int l = 0; l < nlev; l++) {
+                    sh_in -= lr(l);
+                    c0 |= ((slot >> sh_in) & ((1u << lr(l)) - 1)) << sh_out;
+                    sh_out += lr(l);
+                }
+                const uint32_t v = mulmod_c(mulmod_c(powmod_c(g, c0), s_inv), pow_root(ls, (uint64_t)c0 * k2 % S));
+                all.push_back(tw_of(v));
+            }
+    }
+    // NTT levels 1 .. nlev-2: [k2*L + m] = omega_N^(m*k2)
+    int npb = nlr(0);
+    off[3] = all.size();
+    if (nlev >= 3) {
+        const int l = 1;
+        const int logn = ls - npb, R = 1 << nlr(l), L = 1 << (logn - nlr(l));
+        const uint32_t N = 1u << logn;
+        for (int k2 = 0; k2 < R; k2++)
+            for (int m = 0; m < L; m++) all.push_back(tw_of(pow_root(logn, (uint64_t)m * k2 % N)));
+    }
+    off[4] = all.size();
+}
+
 static int log2_exact(uint64_t x) {
     if (x == 0 || (x & (x - 1))) return -1;
     int l = 0;
@@ -139,6 +195,20 @@ zoda_status zoda_ctx_create(int device, zoda_ctx** out) {
         set_last_error("cudaMemcpy(tables)", e);
         return fail(ZODA_ERR_CUDA);
     }
+    if ((e = cudaMalloc(&c->d_err, sizeof(int))) != cudaSuccess || (e = cudaMemset(c->d_err, 0, sizeof(int))) != cudaSuccess) {
+        set_last_error("cudaMalloc(err)", e);
+        return fail(ZODA_ERR_NOMEM);
+    }
+    {
+        std::vector<Tw> side;
+        for (int ls = 7; ls <= 12; ls++) build_side_tables(ls, side, c->tables.side_off[ls]);
+        if ((e = cudaMalloc(&c->tables.side, side.size() * sizeof(Tw))) != cudaSuccess ||
+            (e = cudaMemcpy(c->tables.side, side.data(), side.size() * sizeof(Tw), cudaMemcpyHostToDevice)) !=
+                cudaSuccess) {
+            set_last_error("cudaMalloc(side tables)", e);
+            return fail(ZODA_ERR_NOMEM);
+        }
+    }
     zoda_status s = extend_init_attributes();
     if (s != ZODA_OK) return fail(s);
     *out = c;
@@ -151,8 +221,10 @@ void zoda_ctx_destroy(zoda_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     c->in_buf.release();
     c->out_buf.release();
+    if (c->d_err) cudaFree(c->d_err);
     if (c->tables.tw) cudaFree(c->tables.tw);
     if (c->tables.twist) cudaFree(c->tables.twist);
+    if (c->tables.side) cudaFree(c->tables.side);
     for (auto& ev : c->ev)
         if (ev) cudaEventDestroy(ev);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -182,7 +254,27 @@ zoda_status zoda_extend_device(zoda_ctx* ctx, const uint32_t* d_in, uint32_t* d_
     if (a < b + 2 * in_bytes && b < a + in_bytes) return ZODA_ERR_ARG;  // overlap
     if (cols == 0) return ZODA_OK;
     ZB_CUDA(cudaSetDevice(ctx->device));
-    return launch_extend(ctx, ls, d_in, d_out, cols, (cudaStream_t)stream);
+    return launch_extend(ctx, ls, d_in, d_out, cols, (cudaStream_t)stream, ctx->impl);
+}
+
+zoda_status zoda_ctx_set_impl(zoda_ctx* ctx, int impl) {
+    if (!ctx || impl < 0 || impl > 2) return ZODA_ERR_ARG;
+    ctx->impl = impl;
+    return ZODA_OK;
+}
+
+zoda_status zoda_ctx_check(zoda_ctx* ctx) {
+    if (!ctx) return ZODA_ERR_ARG;
+    ZB_CUDA(cudaSetDevice(ctx->device));
+    ZB_CUDA(cudaDeviceSynchronize());
+    int flag = 0;
+    ZB_CUDA(cudaMemcpy(&flag, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+        ZB_CUDA(cudaMemset(ctx->d_err, 0, sizeof(int)));
+        set_last_error_text("a kernel gave up a bounded wait");
+        return ZODA_ERR_TIMEOUT;
+    }
+    return ZODA_OK;
 }
 
 zoda_status zoda_extend_host(zoda_ctx* ctx, const uint32_t* h_in, uint32_t* h_out, uint32_t k, uint64_t cols,
@@ -199,7 +291,8 @@ zoda_status zoda_extend_host(zoda_ctx* ctx, const uint32_t* h_in, uint32_t* h_ou
     ZB_CUDA(cudaEventRecord(ctx->ev[0], st));
     ZB_CUDA(cudaMemcpyAsync(ctx->in_buf.p, h_in, in_bytes, cudaMemcpyHostToDevice, st));
     ZB_CUDA(cudaEventRecord(ctx->ev[1], st));
-    if ((s = launch_extend(ctx, ls, (const uint32_t*)ctx->in_buf.p, (uint32_t*)ctx->out_buf.p, cols, st)) != ZODA_OK)
+    if ((s = launch_extend(ctx, ls, (const uint32_t*)ctx->in_buf.p, (uint32_t*)ctx->out_buf.p, cols, st,
+                           ctx->impl)) != ZODA_OK)
         return s;
     ZB_CUDA(cudaEventRecord(ctx->ev[2], st));
     ZB_CUDA(cudaMemcpyAsync(h_out, ctx->out_buf.p, out_bytes, cudaMemcpyDeviceToHost, st));

@@ -74,11 +74,12 @@ template <bool INV, int LH, int... Js>
 __device__ __forceinline__ void stage(V4* x, std::integer_sequence<int, Js...>) {
     (bfly_at<INV, LH, Js>(x), ...);
 }
-template <bool INV, int LOG_R, int LH>
+// stages with span 2^LH down to 2^LOW
+template <bool INV, int LOG_R, int LH, int LOW = 0>
 __device__ __forceinline__ void stages(V4* x) {
-    if constexpr (LH >= 0) {
+    if constexpr (LH >= LOW) {
         stage<INV, LH>(x, std::make_integer_sequence<int, (1 << LOG_R)>{});
-        stages<INV, LOG_R, LH - 1>(x);
+        stages<INV, LOG_R, LH - 1, LOW>(x);
     }
 }
 }  // namespace detail

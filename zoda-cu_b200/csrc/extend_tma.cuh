@@ -1,0 +1,466 @@
+// Fused extension, TMA-staged variant for sides 128..4096.
+//
+// Same math and level structure as extend.cuh (INTT DIF levels, twist, NTT DIF
+// levels in mirrored order), organised for latency hiding:
+//   * the CTA's input tile [S rows][C cols] arrives in shared memory by TMA
+//     (cp.async.bulk.tensor, boxes of 256 rows x C columns, C*4 >= 32 bytes of
+//     contiguous row segment per box row); the next tile's load is issued as
+//     soon as every thread has copied the current one into registers, so it
+//     overlaps the whole butterfly phase;
+//   * the even output rows (a copy of the input) leave by TMA store straight
+//     from the staging buffer; the odd rows leave by 16-byte streaming stores;
+//   * the CTA is split into two warp-groups of 256 threads, each owning half of
+//     the tile's column quads with its own exchange buffer and named barrier,
+//     so one group computes while the other waits at a barrier;
+//   * the exchange between levels goes through shared memory in two halves
+//     (columns 0-1, then 2-3 of every quad), which keeps staging + exchange +
+//     twiddle tables inside 227 KB;
+//   * the inter-level twiddles and the twist are folded into each level's last
+//     butterfly stage: a + b and a - b + p lie in [0, 2p), valid Shoup inputs,
+//     so those sums are never reduced on their own.
+#pragma once
+#include <cuda.h>
+
+#include "extend.cuh"
+
+namespace zb {
+
+// ---- PTX helpers ------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: gives up after ~2^22 polls (well over a second) instead of hanging.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (uint32_t i = 0; i < (1u << 22); i++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, int x, int y, const void* src) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(map), "r"(x),
+                 "r"(y), "r"(smem_u32(src))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void group_bar(int id) { asm volatile("bar.sync %0, 256;" ::"r"(id) : "memory"); }
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// OR of a predicate over one warp-group, through its named barrier.
+__device__ __forceinline__ bool group_vote_or(int id, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n .reg .pred p, q;\n setp.ne.u32 q, %2, 0;\n bar.red.or.pred p, %1, 256, q;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(r)
+        : "r"(id), "r"((uint32_t)v)
+        : "memory");
+    return r != 0;
+}
+
+// ---- geometry ------------------------------------------------------------------
+// Shared-memory layouts are chosen so that every warp access is bank-conflict
+// free (checked with a bank model of all access patterns):
+//   * staging: TMA swizzle (128B / 64B / 32B mode for 128 / 64 / 32-byte rows),
+//     16-byte chunk index XOR-ed with row bits, undone when reading; the two
+//     warp-groups own alternating column quads;
+//   * exchange: word(slot, q) = slot*GQ + q + sum PW*(slot >> PS), a padding that
+//     stays additive in the register index, so addresses keep immediate offsets;
+//   * twiddle tables live in HBM/L1 in [k2][index] order (see SideTables).
+// staging-conflict-free lane map for side 1024 (basis images of the 3 low bits)
+constexpr int PERM10_B0 = 5, PERM10_B1 = 2, PERM10_B2 = 1;
+
+template <int LOG_S>
+struct XPad {  // exchange padding word(slot) += PW1*(slot >> PS1) + PW2*(slot >> PS2), per side
+    static constexpr int PS1 = LOG_S == 9 ? 1 : LOG_S == 10 ? 3 : LOG_S == 11 ? 3 : LOG_S == 12 ? 4 : 0;
+    static constexpr int PW1 = LOG_S == 9 ? 1 : LOG_S == 10 ? 8 : LOG_S == 11 ? 2 : LOG_S == 12 ? 1 : 0;
+    static constexpr int PS2 = LOG_S == 10 ? 4 : LOG_S == 11 ? 6 : 0;
+    static constexpr int PW2 = LOG_S == 10 ? 4 : LOG_S == 11 ? 2 : 0;
+};
+
+template <int LOG_S_>
+struct TPlan {
+    using PL = ExtPlan<LOG_S_>;  // whole-CTA view: 512 threads, Q4 quads, C columns
+    static constexpr int LOG_S = LOG_S_;
+    static constexpr int S = PL::S, C = PL::C, Q4 = PL::Q4, TPQ = PL::TPQ, EPT = PL::EPT;
+    static constexpr int NLEV = PL::NLEV;
+    static constexpr int GQ = Q4 / 2;  // quads per warp-group
+    static constexpr int BOX_R = S < 256 ? S : 256;
+    static constexpr int NBOX = S / BOX_R;
+    static constexpr uint32_t TILE_BYTES = (uint32_t)S * C * 4;
+    // staging swizzle: rows of C*4 bytes; 0 = none, else the XOR mask on (offset >> 7)
+    static constexpr int ROW_BYTES = C * 4;
+    static constexpr uint32_t SWZ_MASK = ROW_BYTES == 128 ? 7 : ROW_BYTES == 64 ? 3 : ROW_BYTES == 32 ? 1 : 0;
+    using XP = XPad<LOG_S>;
+    // Lane map inside a warp: quad ql = lane % GQ, row group t = TW*warp + perm(lane / GQ),
+    // perm a bit-linear map (images of the basis vectors) chosen, together with the
+    // exchange padding, so staging reads and every exchange access are conflict free.
+    static constexpr int TW = GQ < 32 ? 32 / GQ : 1;
+    static constexpr int PB0 = LOG_S == 11 ? 1 : LOG_S == 10 ? PERM10_B0 : 1;
+    static constexpr int PB1 = LOG_S == 11 ? 4 : LOG_S == 10 ? PERM10_B1 : 2;
+    static constexpr int PB2 = LOG_S == 11 ? 2 : LOG_S == 10 ? PERM10_B2 : 4;
+    __device__ static __forceinline__ int lane_t(int x) {  // x = lane / GQ in [0, TW)
+        int y = x & ~7;
+        if (x & 1) y ^= PB0;
+        if (x & 2) y ^= PB1;
+        if (x & 4) y ^= PB2;
+        return y;
+    }
+    static constexpr size_t X_WORDS = (size_t)S * GQ + (size_t)XP::PW1 * (S >> XP::PS1) +
+                                      (size_t)XP::PW2 * (XP::PW2 ? (S >> XP::PS2) : 0) + GQ;
+    static constexpr size_t X_BYTES = X_WORDS * 8;  // one group's half-exchange buffer
+    static constexpr size_t OFF_X = TILE_BYTES;
+    static constexpr size_t OFF_BAR = (OFF_X + 2 * X_BYTES + 15) / 16 * 16;
+    static constexpr size_t SMEM = OFF_BAR + 32;
+    static_assert(LOG_S >= 7 && LOG_S <= 12, "TMA path covers sides 128..4096");
+    static_assert(C <= 256 && GQ >= 1, "box inner dimension");
+    static_assert(NLEV >= 2, "at least one exchange");
+    static_assert(SMEM <= 232448, "shared memory budget");
+    static_assert(SWZ_MASK == 0 || (S / 16) * ROW_BYTES % (128 * (SWZ_MASK + 1)) == 0,
+                  "staging row offsets j*L0 must keep the swizzle phase");
+    __host__ __device__ static constexpr int lr(int l) { return PL::lr(l); }
+    __host__ __device__ static constexpr int nlr(int l) { return PL::nlr(l); }
+    __host__ __device__ static constexpr int pre(int l) { return PL::pre(l); }
+    __host__ __device__ static constexpr int npre(int l) { return PL::npre(l); }
+    // padded exchange word offset of a slot (additive over disjoint bit fields)
+    __host__ __device__ static constexpr uint32_t xoff(uint32_t slot) {
+        return slot * GQ + XP::PW1 * (slot >> XP::PS1) + (XP::PW2 ? XP::PW2 * (slot >> XP::PS2) : 0);
+    }
+    __device__ static __forceinline__ uint32_t xword(uint32_t slot, int ql) { return xoff(slot) + (uint32_t)ql; }
+    // staging byte offset of (row, quad)
+    __device__ static __forceinline__ uint32_t stage_off(uint32_t row, int q) {
+        const uint32_t o = row * ROW_BYTES + 16u * (uint32_t)q;
+        if constexpr (SWZ_MASK) return o ^ (((o >> 7) & SWZ_MASK) << 4);
+        return o;
+    }
+};
+
+// Per-side twiddle tables in HBM (read through L1), laid out [k2][index] so a
+// warp's lanes (consecutive group index) read consecutive 8-byte entries:
+//   intt[l][k2*L + m] = omega_N^(-m*k2)      INTT levels 0..NLEV-2
+//   ntt0[k2*NB + b]   = g^c0(b)/S * omega_S^(c0(b)*k2)   NTT level 0 with the twist
+//   ntt[l][k2*L + m]  = omega_N^(m*k2)       NTT levels 1..NLEV-2
+// where level geometry (N, L, R) is that of ExtPlan, b the INTT last-level
+// block, c0(b) its first coefficient index.
+struct SideTables {
+    const uint2* intt[2];
+    const uint2* ntt0;
+    const uint2* ntt[2];
+};
+
+// Twiddle functors: get<K>() returns the factor for output k2 = K.
+template <int L>
+struct TabTw {
+    const uint2* p;  // &table[index]
+    template <int K>
+    __device__ __forceinline__ Tw get() const {
+        const uint2 u = __ldg(p + K * L);
+        return Tw{u.x, u.y};
+    }
+};
+template <int LOG_M, bool INV>
+struct ConstTw {  // omega_{2^LOG_M}^(+-K), an immediate
+    template <int K>
+    __device__ __forceinline__ Tw get() const {
+        constexpr uint32_t w = root_pow(LOG_M, (uint32_t)K, INV);
+        constexpr uint32_t ws = shoup(w);
+        return Tw{w, ws};
+    }
+};
+
+namespace detail {
+template <int LR, bool SKIP0, int I, class TwF>
+__device__ __forceinline__ void pair_twout(V4* x, const TwF& twf) {
+    constexpr int ka = bitrev(I, LR), kb = bitrev(I + 1, LR);
+    const Tw tb = twf.template get<kb>();
+    if constexpr (SKIP0 && ka == 0) {
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const uint32_t a = x[I].c[c], b = x[I + 1].c[c];
+            x[I].c[c] = add_mod(a, b);
+            x[I + 1].c[c] = mul_tw(a - b + P, tb.w, tb.ws);
+        }
+    } else {
+        const Tw ta = twf.template get<ka>();
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const uint32_t a = x[I].c[c], b = x[I + 1].c[c];
+            x[I].c[c] = mul_tw(a + b, ta.w, ta.ws);
+            x[I + 1].c[c] = mul_tw(a - b + P, tb.w, tb.ws);
+        }
+    }
+}
+template <int LR, bool SKIP0, class TwF, int... Is>
+__device__ __forceinline__ void last_stage_twout(V4* x, const TwF& twf, std::integer_sequence<int, Is...>) {
+    (pair_twout<LR, SKIP0, 2 * Is>(x, twf), ...);
+}
+}  // namespace detail
+
+// DIF DFT of size 2^LR whose last (twiddle-free) stage also multiplies output
+// k2 = bitrev(r) by twf.get<k2>(); a + b and a - b + p lie in [0, 2p), valid
+// Shoup inputs, so those sums are never reduced on their own. With SKIP0 the
+// output k2 = 0 has factor 1 and is only reduced.
+template <int LR, bool INV, bool SKIP0, class TwF>
+__device__ __forceinline__ void dft_dif_twout(V4* x, const TwF& twf) {
+    if constexpr (LR > 1) detail::stages<INV, LR, LR - 1, 1>(x);
+    detail::last_stage_twout<LR, SKIP0>(x, twf, std::make_integer_sequence<int, (1 << LR) / 2>{});
+}
+
+// Level geometry (as ExtPlan): 2^PB blocks of N = 2^LOGN slots, slot = block*N |
+// n1 | (j << LOGL); the thread's group g is gid = g*TPQ + t.
+template <class TP, int LR, int PB>
+struct LvlGeom {
+    static constexpr int R = 1 << LR;
+    static constexpr int G = TP::EPT / R;
+    static constexpr int LOGN = TP::LOG_S - PB;
+    static constexpr int LOGL = LOGN - LR;
+    static constexpr int L = 1 << LOGL;
+    __device__ static __forceinline__ uint32_t gid(int g, int t) { return (uint32_t)(g * TP::TPQ + t); }
+    __device__ static __forceinline__ uint32_t base(uint32_t id) {
+        return ((id >> LOGL) << LOGN) | (id & ((1u << LOGL) - 1));
+    }
+    __device__ static __forceinline__ uint32_t n1(uint32_t id) { return id & ((1u << LOGL) - 1); }
+};
+
+// Exchange through one group's half buffer. The writer's output register
+// g*RW + r (DFT output k2 = bitrev(r)) sits at slot wbase(g) | (k2 << WSH); the
+// reader's input register g*RR + j at slot rbase(g) | (j << RSH). The base and
+// the shifted index occupy disjoint bits, so each padded word address is a
+// per-group base plus a compile-time offset. Columns 0-1 go first, then 2-3.
+template <class TP, int RW, int WSH, int RR, int RSH, class WB, class RBs>
+__device__ __forceinline__ void exchange(V4* v, uint2* xg, int ql, int bar, const WB& wbase, const RBs& rbase) {
+    constexpr int GW = TP::EPT / RW, GR = TP::EPT / RR;
+    constexpr int LRW = RW == 1 ? 0 : RW == 2 ? 1 : RW == 4 ? 2 : RW == 8 ? 3 : 4;
+    uint32_t wb[GW], rb[GR];
+#pragma unroll
+    for (int g = 0; g < GW; g++) wb[g] = TP::xword(wbase(g), ql);
+#pragma unroll
+    for (int g = 0; g < GR; g++) rb[g] = TP::xword(rbase(g), ql);
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        group_bar(bar);
+#pragma unroll
+        for (int g = 0; g < GW; g++)
+#pragma unroll
+            for (int r = 0; r < RW; r++)
+                xg[wb[g] + TP::xoff((uint32_t)bitrev(r, LRW) << WSH)] =
+                    make_uint2(v[g * RW + r].c[2 * h], v[g * RW + r].c[2 * h + 1]);
+        group_bar(bar);
+#pragma unroll
+        for (int g = 0; g < GR; g++)
+#pragma unroll
+            for (int j = 0; j < RR; j++) {
+                const uint2 u = xg[rb[g] + TP::xoff((uint32_t)j << RSH)];
+                v[g * RR + j].c[2 * h] = u.x;
+                v[g * RR + j].c[2 * h + 1] = u.y;
+            }
+    }
+}
+
+// INTT levels l .. NLEV-2 (each followed by an exchange); the last INTT level is
+// run by the kernel body.
+template <class TP, int l>
+__device__ __forceinline__ void intt_upto_last(V4* v, uint2* xg, int t, int ql, int bar, const SideTables& tb) {
+    if constexpr (l < TP::NLEV - 1) {
+        using W = LvlGeom<TP, TP::lr(l), TP::pre(l)>;
+        using Rd = LvlGeom<TP, TP::lr(l + 1), TP::pre(l + 1)>;
+#pragma unroll
+        for (int g = 0; g < W::G; g++) {
+            const TabTw<W::L> twf{tb.intt[l] + W::n1(W::gid(g, t))};
+            dft_dif_twout<TP::lr(l), true, true>(v + g * W::R, twf);
+        }
+        exchange<TP, W::R, W::LOGL, Rd::R, Rd::LOGL>(
+            v, xg, ql, bar, [&](int g) { return W::base(W::gid(g, t)); },
+            [&](int g) { return Rd::base(Rd::gid(g, t)); });
+        intt_upto_last<TP, l + 1>(v, xg, t, ql, bar, tb);
+    }
+}
+
+// NTT levels l .. NLEV-1 (level 0 runs in the kernel body); the last one stores
+// the odd output rows.
+template <class TP, int l>
+__device__ __forceinline__ void ntt_from(V4* v, uint2* xg, int t, int ql, int bar, const SideTables& tb,
+                                         uint32_t* __restrict__ out, uint64_t cols, uint64_t col, bool active) {
+    using LV = LvlGeom<TP, TP::nlr(l), TP::npre(l)>;
+    if constexpr (l < TP::NLEV - 1) {
+        using Rd = LvlGeom<TP, TP::nlr(l + 1), TP::npre(l + 1)>;
+#pragma unroll
+        for (int g = 0; g < LV::G; g++) {
+            const TabTw<LV::L> twf{tb.ntt[l] + LV::n1(LV::gid(g, t))};
+            dft_dif_twout<TP::nlr(l), false, true>(v + g * LV::R, twf);
+        }
+        exchange<TP, LV::R, LV::LOGL, Rd::R, Rd::LOGL>(
+            v, xg, ql, bar, [&](int g) { return LV::base(LV::gid(g, t)); },
+            [&](int g) { return Rd::base(Rd::gid(g, t)); });
+        ntt_from<TP, l + 1>(v, xg, t, ql, bar, tb, out, cols, col, active);
+    } else {
+#pragma unroll
+        for (int g = 0; g < LV::G; g++) dft_dif<TP::nlr(l), false>(v + g * LV::R);
+#pragma unroll
+        for (int g = 0; g < LV::G; g++) {
+            const uint32_t blk = LV::gid(g, t);
+#pragma unroll
+            for (int r = 0; r < LV::R; r++) {
+                const uint32_t k =
+                    digit_rev<typename TP::PL, true>((blk << TP::nlr(l)) | (uint32_t)bitrev(r, TP::nlr(l)));
+                if (active) stg_stream_v4(out + (2 * (uint64_t)k + 1) * cols + col, v[g * LV::R + r]);
+            }
+        }
+    }
+}
+
+template <int LOG_S>
+__global__ void __launch_bounds__(512, 1)
+    k_extend_tma(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_even,
+                 uint32_t* __restrict__ out, uint64_t cols, uint64_t ntiles, const SideTables tb,
+                 int* __restrict__ err) {
+    using TP = TPlan<LOG_S>;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    uint32_t* stage = reinterpret_cast<uint32_t*>(smem);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + TP::OFF_BAR);   // tile landed (TMA tx)
+    uint64_t* empty = full + 1;                                          // both groups copied it out
+    const int tid = threadIdx.x;
+    const int grp = tid >> 8;
+    const int bar = 1 + grp;
+    // Thread 256 (first thread of group 1, the group that reads the staging
+    // buffer last) is the producer: it issues every TMA load and even-row store.
+    const bool producer = tid == 256;
+    if (tid == 0) {
+        mbar_init(full, 1);
+        mbar_init(empty, 2);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    uint64_t tile = blockIdx.x;
+    if (producer && tile < ntiles) {
+        mbar_expect_tx(full, TP::TILE_BYTES);
+#pragma unroll
+        for (int b = 0; b < TP::NBOX; b++)
+            tma_load_2d(stage + (size_t)b * TP::BOX_R * TP::C, &tm_in, (int)(tile * TP::C), b * TP::BOX_R, full);
+    }
+    // Group 1 starts half a tile after group 0 so the two groups' barriers and
+    // butterfly phases interleave; group 0 signals from the middle of its first tile.
+    if (grp == 1 && tile < ntiles) asm volatile("bar.sync 3, 512;" ::: "memory");
+    bool stagger_pending = grp == 0;
+    V4 v[TP::EPT];
+    uint32_t parity = 0;
+    for (; tile < ntiles; tile += gridDim.x, parity ^= 1) {
+        // Thread coordinates are re-derived each tile from an opaque copy of tid so
+        // the compiler rebuilds the per-pattern smem addresses here instead of
+        // keeping them all live across the loop.
+        int tid_l;
+        asm volatile("mov.u32 %0, %1;" : "=r"(tid_l) : "r"(tid));
+        const int ltid = tid_l & 255;
+        const int lane = ltid & 31, wg = ltid >> 5;
+        const int ql = TP::GQ < 32 ? lane % TP::GQ : ltid % TP::GQ;
+        const int t = TP::GQ < 32 ? wg * TP::TW + TP::lane_t(lane / TP::GQ) : ltid / TP::GQ;
+        const int q = grp * TP::GQ + ql;
+        uint2* xg = reinterpret_cast<uint2*>(smem + TP::OFF_X + (tid_l >> 8) * TP::X_BYTES);
+        const bool ok = mbar_wait_bounded(full, parity);
+        if (group_vote_or(bar, !ok)) {
+            if ((tid & 255) == 0) atomicOr(err, 1);
+            if (stagger_pending) asm volatile("bar.arrive 3, 512;" ::: "memory");
+            if (producer) bulk_wait0();
+            return;
+        }
+        if (producer) {  // even output rows = the input tile, straight from staging
+#pragma unroll
+            for (int b = 0; b < TP::NBOX; b++)
+                tma_store_2d(&tm_even, (int)(tile * TP::C), b * TP::BOX_R, stage + (size_t)b * TP::BOX_R * TP::C);
+            bulk_commit();
+        }
+        const uint64_t col = tile * TP::C + 4 * (uint64_t)q;
+        const bool active = col < cols;
+        {
+            constexpr int R0 = 1 << TP::lr(0);
+            constexpr int L0 = TP::S / R0;
+            const unsigned char* sb = smem + TP::stage_off((uint32_t)t, q);
+#pragma unroll
+            for (int j = 0; j < R0; j++) {
+                const uint4 u = *reinterpret_cast<const uint4*>(sb + (size_t)j * L0 * TP::ROW_BYTES);
+                v[j] = V4{{u.x, u.y, u.z, u.w}};
+            }
+        }
+        group_bar(bar);  // this group has copied the staging buffer out
+        if ((tid & 255) == 0) mbar_arrive(empty);
+        const uint64_t next = tile + gridDim.x;
+        if (producer && next < ntiles) {
+            const bool e_ok = mbar_wait_bounded(empty, parity);  // the other group is done too
+            bulk_wait_read0();  // the even-row store has finished reading staging
+            fence_proxy_async();
+            if (e_ok) {
+                mbar_expect_tx(full, TP::TILE_BYTES);
+#pragma unroll
+                for (int b = 0; b < TP::NBOX; b++)
+                    tma_load_2d(stage + (size_t)b * TP::BOX_R * TP::C, &tm_in, (int)(next * TP::C),
+                                b * TP::BOX_R, full);
+            } else {
+                atomicOr(err, 2);  // both groups then time out on `full` and leave
+            }
+        }
+
+        // ---- INTT levels 0 .. NLEV-2
+        intt_upto_last<TP, 0>(v, xg, t, ql, bar, tb);
+        if (stagger_pending) {
+            asm volatile("bar.arrive 3, 512;" ::: "memory");
+            stagger_pending = false;
+        }
+        {
+            // ---- INTT last level (L = 1). Its outputs need the twist g^c / S with
+            // c = c0 + k2*S/R; g^(k2*S/R) = omega_2R^k2 is an immediate folded into the
+            // last butterfly stage, and g^c0 / S is folded into NTT level 0's table.
+            constexpr int LR = TP::lr(TP::NLEV - 1);
+            constexpr int R = 1 << LR;
+            constexpr int G = TP::EPT / R;
+            constexpr int NB = TP::S / R;  // INTT last-level blocks
+            constexpr int SH = TP::LOG_S - LR;
+            using LV = LvlGeom<TP, LR, TP::pre(TP::NLEV - 1)>;
+            using Rd = LvlGeom<TP, TP::nlr(1), TP::npre(1)>;
+#pragma unroll
+            for (int g = 0; g < G; g++) {
+                dft_dif_twout<LR, true, true>(v + g * R, ConstTw<LR + 1, false>{});
+                // NTT level 0 wants coefficient c0 + (S/R)*j in register j
+                V4 y[R];
+#pragma unroll
+                for (int j = 0; j < R; j++) y[j] = v[g * R + bitrev(j, LR)];
+#pragma unroll
+                for (int j = 0; j < R; j++) v[g * R + j] = y[j];
+                // ---- NTT level 0: radix R over stride S/R, then g^c0/S * omega_S^(c0*k2)
+                const TabTw<NB> twf{tb.ntt0 + LV::gid(g, t)};
+                dft_dif_twout<LR, false, false>(v + g * R, twf);
+            }
+            exchange<TP, R, SH, Rd::R, Rd::LOGL>(
+                v, xg, ql, bar, [&](int g) { return digit_rev<typename TP::PL, false>(LV::gid(g, t) << LR); },
+                [&](int g) { return Rd::base(Rd::gid(g, t)); });
+        }
+        // ---- NTT levels 1 .. NLEV-1, the last one stores the odd rows
+        ntt_from<TP, 1>(v, xg, t, ql, bar, tb, out, cols, col, active);
+    }
+    if (stagger_pending) asm volatile("bar.arrive 3, 512;" ::: "memory");
+    if (producer) bulk_wait0();
+}
+
+}  // namespace zb

@@ -51,20 +51,22 @@ __host__ __device__ constexpr uint32_t root_pow(int log_n, uint32_t e, bool inv)
 }
 
 // ---- device arithmetic -----------------------------------------------------
+// The reductions use the DPX instruction VIADDMNMX (min(a + b, c) in one issue
+// slot, native on sm_100a): a modular add is IADD3 + VIADDMNMX, a reduction
+// from [0, 2p) a single VIADDMNMX.
 __device__ __forceinline__ uint32_t add_mod(uint32_t a, uint32_t b) {  // a, b in [0, p)
-    uint32_t s = a + b;
-    return min(s, s - P);
+    return __viaddmin_u32(a, b, a + b - P);
 }
 __device__ __forceinline__ uint32_t sub_mod(uint32_t a, uint32_t b) {  // a, b in [0, p)
-    uint32_t d = a - b;
-    return min(d, d + P);
+    const uint32_t d = a - b;
+    return __viaddmin_u32(d, P, d);
 }
 __device__ __forceinline__ uint32_t reduce_2p(uint32_t r) {  // r in [0, 2p) -> [0, p)
-    return min(r, r - P);
+    return __viaddmin_u32(r, 0u - P, r);
 }
 // x any u32 -> x*w mod p, in [0, 2p)
 __device__ __forceinline__ uint32_t mul_lazy(uint32_t x, uint32_t w, uint32_t ws) {
-    uint32_t q = __umulhi(x, ws);
+    const uint32_t q = __umulhi(x, ws);
     return x * w - q * P;
 }
 __device__ __forceinline__ uint32_t mul_tw(uint32_t x, uint32_t w, uint32_t ws) {
@@ -85,12 +87,19 @@ __device__ __forceinline__ void dif_bfly(uint32_t& a, uint32_t& b, uint32_t w, u
     a = x;
     b = y;
 }
-// Twiddle-free DIF butterfly: (a, b) -> (a + b, a - b).
+// Twiddle-free DIF butterfly: (a, b) -> (a + b, a - b). The unreduced sum and
+// difference are formed with IMAD (x*1 + y, x*(2^32-1) + y) so this butterfly
+// loads the FMA pipe as much as the ALU pipe: the twiddled butterflies are
+// ALU-light, these would otherwise be ALU-only and the ALU pipe would bind.
+// The multipliers 1 and 2^32-1 live in constant memory, which the assembler
+// cannot see through, so it keeps the IMADs instead of rewriting them as adds.
+__constant__ uint32_t c_imad_one = 1u;
+__constant__ uint32_t c_imad_neg1 = 0xFFFFFFFFu;
 __device__ __forceinline__ void dif_bfly1(uint32_t& a, uint32_t& b) {
-    uint32_t x = add_mod(a, b);
-    uint32_t y = sub_mod(a, b);
-    a = x;
-    b = y;
+    const uint32_t u = a * c_imad_one + b;     // a + b, IMAD
+    const uint32_t d = b * c_imad_neg1 + a;    // a - b (mod 2^32), IMAD
+    a = __viaddmin_u32(u, 0u - P, u);             // min(u - p, u)
+    b = __viaddmin_u32(d, P, d);                  // min(d + p, d)
 }
 
 struct Tw {  // twiddle and its Shoup companion

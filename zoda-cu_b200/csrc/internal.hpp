@@ -38,6 +38,9 @@ struct DevBuf {
 struct Tables {
     Tw* tw = nullptr;
     Tw* twist = nullptr;
+    // per-side level tables of the TMA-staged kernel (log2 side 7..12), one buffer
+    Tw* side = nullptr;
+    size_t side_off[13][5] = {};  // [log_s][intt0, intt1, ntt0, ntt1, end] entry offsets
 };
 
 }  // namespace zb
@@ -47,6 +50,8 @@ struct zoda_ctx {
     int sm_count = 0;
     cudaStream_t stream = nullptr;
     zb::Tables tables;
+    int* d_err = nullptr;  // device flag a kernel sets when a bounded wait gives up
+    int impl = 0;          // zoda_extend_impl
     // host-call staging
     zb::DevBuf in_buf, out_buf;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -55,8 +60,9 @@ struct zoda_ctx {
 
 namespace zb {
 // Launches the fused extension kernel for side 2^log_s (0 <= log_s <= 12).
+// impl: 0 = automatic, 1 = direct-load kernel, 2 = TMA-staged kernel (sides 128..4096).
 zoda_status launch_extend(const zoda_ctx* ctx, int log_s, const uint32_t* in, uint32_t* out, uint64_t cols,
-                          cudaStream_t st);
+                          cudaStream_t st, int impl = 0);
 // Sets the dynamic shared memory attribute of every extension instantiation.
 zoda_status extend_init_attributes();
 }  // namespace zb

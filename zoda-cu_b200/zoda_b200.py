@@ -31,7 +31,7 @@ STATUS = {
 EXPORTS = [
     "cuda_ntt", "cuda_intt", "cuda_host_alloc", "cuda_host_free",
     "zoda_status_string", "zoda_last_error", "zoda_ctx_create", "zoda_ctx_destroy", "zoda_max_side",
-    "zoda_extend_device", "zoda_extend_host",
+    "zoda_extend_device", "zoda_extend_host", "zoda_ctx_set_impl", "zoda_ctx_check",
 ]
 
 _lib = None
@@ -78,6 +78,10 @@ def load(path: str = LIB_PATH):
     L.zoda_max_side.argtypes = []
     L.zoda_extend_device.restype = ctypes.c_int
     L.zoda_extend_device.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.c_uint64, vp]
+    L.zoda_ctx_set_impl.restype = ctypes.c_int
+    L.zoda_ctx_set_impl.argtypes = [vp, ctypes.c_int]
+    L.zoda_ctx_check.restype = ctypes.c_int
+    L.zoda_ctx_check.argtypes = [vp]
     L.zoda_extend_host.restype = ctypes.c_int
     L.zoda_extend_host.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(ZodaTiming)]
     del u32p
@@ -137,6 +141,14 @@ class Context:
         s = stream if isinstance(stream, int) else stream.cuda_stream
         _check(load().zoda_extend_device(self._h, _addr(d_in), _addr(d_out), k, cols, s or None),
                "zoda_extend_device")
+
+    def set_impl(self, impl: int):
+        """0 = automatic, 1 = direct-load kernel, 2 = TMA-staged kernel."""
+        _check(load().zoda_ctx_set_impl(self._h, impl), "zoda_ctx_set_impl")
+
+    def check(self):
+        """Raise if a kernel on this context gave up a bounded wait (synchronizes)."""
+        _check(load().zoda_ctx_check(self._h), "zoda_ctx_check")
 
     def extend_host(self, h_in, h_out, k: int, cols: int) -> ZodaTiming:
         t = ZodaTiming()
