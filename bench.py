@@ -207,6 +207,12 @@ def run_reference(args, world, rank):
 # our arm
 # ---------------------------------------------------------------------------
 
+def kernel_name(side: int) -> str:
+    """The kernel zoda_extend_device launches for this side (automatic variant)."""
+    ls = side.bit_length() - 1
+    return f"k_extend_tma<{ls}>" if 7 <= ls <= 11 else f"k_extend<{ls}>"
+
+
 def time_device_extend(ctx, side: int, steps: int, warmup: int, world: int, sampler=None):
     """Device-resident extension of one side x side square per step, CUDA events on the launching stream."""
     import torch
@@ -362,7 +368,7 @@ def run_ours(args, world, rank, local):
                        "l2": "inputs (and outputs) larger than the 126 MB L2; no flush"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
-                         "peak_source": peaks["source"], "kernel": f"k_extend<{side.bit_length() - 1}>",
+                         "peak_source": peaks["source"], "kernel": kernel_name(side),
                          "alg_bytes_per_launch": alg_bytes},
             "cpu_baseline": cpu,
             "e2e": e2e,

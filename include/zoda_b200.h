@@ -114,20 +114,23 @@ zoda_status zoda_ctx_check(zoda_ctx* ctx);
 zoda_status zoda_extend_device(zoda_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t k, uint64_t cols,
                                void* stream);
 
-/* Timing of a host-buffer call, in milliseconds (CUDA events). */
+/* Timing of a host-buffer call, in milliseconds (CUDA events). The copies
+ * and kernels of different column chunks overlap, so the three busy times
+ * can add up to more than total_ms. */
 typedef struct zoda_timing {
-    float h2d_ms;    /* host -> device copy of the input        */
-    float kernel_ms; /* the fused extension kernel              */
-    float d2h_ms;    /* device -> host copy of the output       */
-    float total_ms;  /* first copy start to last copy end       */
+    float h2d_ms;    /* host -> device copies of the input, summed  */
+    float kernel_ms; /* fused extension kernels, summed             */
+    float d2h_ms;    /* device -> host copies of the output, summed */
+    float total_ms;  /* first copy start to last copy end           */
 } zoda_timing;
 
 /* Fused extension from host memory to host memory: the reference's
  * `encode_gpu` window (src/benchmarks/utils.rs:100-146) without the host
  * transpose and padding, which the kernel makes unnecessary. h_in row-major
  * [k][cols], h_out row-major [2k][cols]; pinned buffers give full PCIe speed.
- * Device buffers are taken from the context's cache. Synchronous.
- * `timing` may be NULL. */
+ * The square moves in column chunks over three streams, so uploads,
+ * kernels and downloads overlap; device buffers are the context's cached
+ * chunk buffers. Synchronous. `timing` may be NULL. */
 zoda_status zoda_extend_host(zoda_ctx* ctx, const uint32_t* h_in, uint32_t* h_out, uint32_t k, uint64_t cols,
                              zoda_timing* timing);
 

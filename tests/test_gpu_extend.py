@@ -136,8 +136,9 @@ def test_extend_erasure_recovery(ctx):
     assert np.array_equal(rec, data)
 
 
-def test_extend_host_matches_device(ctx):
-    side, cols = 256, 4096
+@pytest.mark.parametrize("side,cols", [(256, 4096), (512, 512 * 128 + 4 * 37)])
+def test_extend_host_matches_device(ctx, side, cols):
+    # the second case moves ~134 MB in three column chunks over three streams, the last one ragged
     data = O.seeded_input(side, cols, seed=9)
     h_in = torch.from_numpy(data.view(np.int32)).pin_memory()
     h_out = torch.empty((2 * side, cols), dtype=torch.int32).pin_memory()

@@ -219,8 +219,15 @@ void zoda_ctx_destroy(zoda_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    c->in_buf.release();
-    c->out_buf.release();
+    for (int i = 0; i < zoda_ctx::NHS; i++) {
+        if (c->hs[i]) cudaStreamSynchronize(c->hs[i]);
+        c->hin[i].release();
+        c->hout[i].release();
+        if (c->hs[i]) cudaStreamDestroy(c->hs[i]);
+    }
+    for (auto& row : c->cev)
+        for (auto& e : row)
+            if (e) cudaEventDestroy(e);
     if (c->d_err) cudaFree(c->d_err);
     if (c->tables.tw) cudaFree(c->tables.tw);
     if (c->tables.twist) cudaFree(c->tables.twist);
@@ -284,24 +291,66 @@ zoda_status zoda_extend_host(zoda_ctx* ctx, const uint32_t* h_in, uint32_t* h_ou
     if (s != ZODA_OK) return s;
     std::lock_guard<std::mutex> lock(ctx->mu);
     ZB_CUDA(cudaSetDevice(ctx->device));
-    const size_t in_bytes = (size_t)k * cols * 4, out_bytes = 2 * in_bytes;
-    if ((s = ctx->in_buf.ensure(in_bytes)) != ZODA_OK) return s;
-    if ((s = ctx->out_buf.ensure(out_bytes)) != ZODA_OK) return s;
-    cudaStream_t st = ctx->stream;
-    ZB_CUDA(cudaEventRecord(ctx->ev[0], st));
-    ZB_CUDA(cudaMemcpyAsync(ctx->in_buf.p, h_in, in_bytes, cudaMemcpyHostToDevice, st));
-    ZB_CUDA(cudaEventRecord(ctx->ev[1], st));
-    if ((s = launch_extend(ctx, ls, (const uint32_t*)ctx->in_buf.p, (uint32_t*)ctx->out_buf.p, cols, st,
-                           ctx->impl)) != ZODA_OK)
-        return s;
-    ZB_CUDA(cudaEventRecord(ctx->ev[2], st));
-    ZB_CUDA(cudaMemcpyAsync(h_out, ctx->out_buf.p, out_bytes, cudaMemcpyDeviceToHost, st));
-    ZB_CUDA(cudaEventRecord(ctx->ev[3], st));
+    if (cols == 0) {
+        if (timing) *timing = zoda_timing{0, 0, 0, 0};
+        return ZODA_OK;
+    }
+    // Column chunks of ~64 MiB input rotate over NHS streams, so the upload of
+    // one chunk, the kernel of another and the download of a third overlap
+    // (the two copy directions run on separate engines).
+    const uint64_t in_bytes = (uint64_t)k * cols * 4;
+    uint64_t nch = (in_bytes + (64ull << 20) - 1) / (64ull << 20);
+    if (nch > (uint64_t)zoda_ctx::MAX_CHUNKS) nch = zoda_ctx::MAX_CHUNKS;
+    if (nch > cols / 4) nch = cols / 4 ? cols / 4 : 1;
+    uint64_t cw = (cols + nch - 1) / nch;
+    cw = (cw + 3) & ~3ull;
+    nch = (cols + cw - 1) / cw;
+    for (int i = 0; i < zoda_ctx::NHS; i++) {
+        if (!ctx->hs[i]) ZB_CUDA(cudaStreamCreateWithFlags(&ctx->hs[i], cudaStreamNonBlocking));
+        if ((s = ctx->hin[i].ensure((size_t)k * cw * 4)) != ZODA_OK) return s;
+        if ((s = ctx->hout[i].ensure((size_t)2 * k * cw * 4)) != ZODA_OK) return s;
+    }
+    for (uint64_t c = 0; c < nch; c++)
+        for (auto& e : ctx->cev[c])
+            if (!e) ZB_CUDA(cudaEventCreate(&e));
+    // all streams start after ev[0]
+    ZB_CUDA(cudaEventRecord(ctx->ev[0], ctx->hs[0]));
+    for (int i = 1; i < zoda_ctx::NHS; i++) ZB_CUDA(cudaStreamWaitEvent(ctx->hs[i], ctx->ev[0], 0));
+    for (uint64_t c = 0; c < nch; c++) {
+        const int b = (int)(c % zoda_ctx::NHS);
+        cudaStream_t st = ctx->hs[b];
+        const uint64_t c0 = c * cw, w = (cols - c0 < cw) ? cols - c0 : cw;
+        uint32_t* din = (uint32_t*)ctx->hin[b].p;
+        uint32_t* dout = (uint32_t*)ctx->hout[b].p;
+        cudaEvent_t* e = ctx->cev[c];
+        ZB_CUDA(cudaEventRecord(e[0], st));
+        ZB_CUDA(cudaMemcpy2DAsync(din, w * 4, h_in + c0, cols * 4, w * 4, k, cudaMemcpyHostToDevice, st));
+        ZB_CUDA(cudaEventRecord(e[1], st));
+        if ((s = launch_extend(ctx, ls, din, dout, w, st, ctx->impl)) != ZODA_OK) return s;
+        ZB_CUDA(cudaEventRecord(e[2], st));
+        ZB_CUDA(cudaMemcpy2DAsync(h_out + c0, cols * 4, dout, w * 4, w * 4, 2 * (size_t)k, cudaMemcpyDeviceToHost,
+                                  st));
+        ZB_CUDA(cudaEventRecord(e[3], st));
+    }
+    for (int i = 1; i < zoda_ctx::NHS; i++) {
+        ZB_CUDA(cudaEventRecord(ctx->ev[1], ctx->hs[i]));
+        ZB_CUDA(cudaStreamWaitEvent(ctx->hs[0], ctx->ev[1], 0));
+    }
+    ZB_CUDA(cudaEventRecord(ctx->ev[3], ctx->hs[0]));
     ZB_CUDA(cudaEventSynchronize(ctx->ev[3]));
     if (timing) {
-        ZB_CUDA(cudaEventElapsedTime(&timing->h2d_ms, ctx->ev[0], ctx->ev[1]));
-        ZB_CUDA(cudaEventElapsedTime(&timing->kernel_ms, ctx->ev[1], ctx->ev[2]));
-        ZB_CUDA(cudaEventElapsedTime(&timing->d2h_ms, ctx->ev[2], ctx->ev[3]));
+        float h = 0, kk = 0, d = 0, x = 0;
+        for (uint64_t c = 0; c < nch; c++) {
+            ZB_CUDA(cudaEventElapsedTime(&x, ctx->cev[c][0], ctx->cev[c][1]));
+            h += x;
+            ZB_CUDA(cudaEventElapsedTime(&x, ctx->cev[c][1], ctx->cev[c][2]));
+            kk += x;
+            ZB_CUDA(cudaEventElapsedTime(&x, ctx->cev[c][2], ctx->cev[c][3]));
+            d += x;
+        }
+        timing->h2d_ms = h;
+        timing->kernel_ms = kk;
+        timing->d2h_ms = d;
         ZB_CUDA(cudaEventElapsedTime(&timing->total_ms, ctx->ev[0], ctx->ev[3]));
     }
     return ZODA_OK;

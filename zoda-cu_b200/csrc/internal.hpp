@@ -52,9 +52,14 @@ struct zoda_ctx {
     zb::Tables tables;
     int* d_err = nullptr;  // device flag a kernel sets when a bounded wait gives up
     int impl = 0;          // zoda_extend_impl
-    // host-call staging
-    zb::DevBuf in_buf, out_buf;
+    // host-call staging: NHS streams, one input and one output buffer each, and
+    // 4 timing events per chunk for up to MAX_CHUNKS chunks
+    static constexpr int NHS = 3;
+    static constexpr int MAX_CHUNKS = 64;
+    cudaStream_t hs[NHS] = {nullptr, nullptr, nullptr};
+    zb::DevBuf hin[NHS], hout[NHS];
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t cev[MAX_CHUNKS][4] = {};
     std::mutex mu;  // serialises host calls on one context
 };
 
