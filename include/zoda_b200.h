@@ -134,6 +134,43 @@ typedef struct zoda_timing {
 zoda_status zoda_extend_host(zoda_ctx* ctx, const uint32_t* h_in, uint32_t* h_out, uint32_t k, uint64_t cols,
                              zoda_timing* timing);
 
+/* ======================================================================
+ * Part 3: a transform for callers that cannot allocate device memory
+ * ====================================================================== */
+
+/* No counterpart in the reference: the reference allocates device memory on
+ * every call (cuda/ntt_kernel.cu:111-121).
+ *
+ * For callers that may not allocate device memory while they run: device
+ * memory owned by a pool allocator that forbids raw cudaMalloc, or a
+ * latency-bound path where cudaMalloc/cudaFree would synchronise the device
+ * and stall other streams. The call performs no cudaMalloc, no cudaFree and
+ * no allocating library call; the caller passes the input and the output.
+ *
+ * What it computes: the cuda_ntt (inverse = 0) or cuda_intt (inverse = 1)
+ * transform, with the standard roots [w^0 .. w^(n-1)], w = 31^((p-1)/n), of
+ * `polys` polynomials of n canonical u32 each, laid end to end in device
+ * memory (polynomial c at d_in[c*n .. c*n + n)), written the same way to
+ * d_out (d_out may equal d_in). n must be a power of two <= 4096.
+ * Asynchronous on `stream` (NULL = the legacy default stream).
+ *
+ * Limits: the working copy lives in a fixed 16 MiB device array inside the
+ * library, so n * round_up(polys, 4) must be <= 4194304 u32; larger requests
+ * return ZODA_ERR_UNSUPPORTED with the reason in zoda_last_error(). Every GPU
+ * that loads the library holds that array (and a 64 KiB twiddle table) until
+ * the process exits.
+ *
+ * Set-up: the first call on each device (with that device current) looks up
+ * the arrays' device addresses and uploads the twiddle table, synchronously;
+ * make that first call before capturing any stream into a CUDA graph.
+ *
+ * Concurrency: all calls on a device share the one array and it keeps the
+ * last call's contents. Calls whose work can overlap on the GPU (different
+ * streams, or different host threads, without ordering between them) race and
+ * corrupt each other's results; order them on one stream or with events. */
+zoda_status zoda_ntt_device_noalloc(const uint32_t* d_in, uint32_t* d_out, uint32_t n, uint32_t polys, int inverse,
+                                    void* stream);
+
 #ifdef __cplusplus
 }
 #endif

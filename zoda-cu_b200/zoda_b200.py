@@ -32,6 +32,7 @@ EXPORTS = [
     "cuda_ntt", "cuda_intt", "cuda_host_alloc", "cuda_host_free",
     "zoda_status_string", "zoda_last_error", "zoda_ctx_create", "zoda_ctx_destroy", "zoda_max_side",
     "zoda_extend_device", "zoda_extend_host", "zoda_ctx_set_impl", "zoda_ctx_check",
+    "zoda_ntt_device_noalloc",
 ]
 
 _lib = None
@@ -82,6 +83,8 @@ def load(path: str = LIB_PATH):
     L.zoda_ctx_set_impl.argtypes = [vp, ctypes.c_int]
     L.zoda_ctx_check.restype = ctypes.c_int
     L.zoda_ctx_check.argtypes = [vp]
+    L.zoda_ntt_device_noalloc.restype = ctypes.c_int
+    L.zoda_ntt_device_noalloc.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, vp]
     L.zoda_extend_host.restype = ctypes.c_int
     L.zoda_extend_host.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(ZodaTiming)]
     del u32p
