@@ -134,6 +134,43 @@ typedef struct zoda_timing {
 zoda_status zoda_extend_host(zoda_ctx* ctx, const uint32_t* h_in, uint32_t* h_out, uint32_t k, uint64_t cols,
                              zoda_timing* timing);
 
+/* ----------------------------------------------------------------------
+ * Batched extension: many squares of mixed sides in one persistent launch.
+ * No reference counterpart; the reference encodes one square per call
+ * (src/benchmarks/utils.rs:100-146).
+ * ---------------------------------------------------------------------- */
+
+/* One square of a batch: d_in row-major [k][cols], d_out row-major [2k][cols],
+ * device memory, 16-byte aligned; k a power of two in [32, 2048], cols a
+ * multiple of 4. */
+typedef struct zoda_square {
+    const uint32_t* d_in;
+    uint32_t* d_out;
+    uint32_t k;
+    uint32_t reserved; /* 0 */
+    uint64_t cols;
+} zoda_square;
+
+typedef struct zoda_batch zoda_batch;
+
+/* Plans a batch on `ctx`: sorts the squares by decreasing side, builds their
+ * TMA descriptors and the (square, column tile) work queue in device memory.
+ * The buffers are not touched until zoda_batch_run. */
+zoda_status zoda_batch_create(zoda_ctx* ctx, const zoda_square* squares, uint32_t n, zoda_batch** out);
+
+/* Encodes every square of the batch with one persistent kernel whose CTAs
+ * (one per SM) take (square, column tile) items from a device counter, big
+ * squares first. The first call captures the counter reset and the launch
+ * into a CUDA graph; every call replays that graph on `stream` (a
+ * cudaStream_t, NULL = legacy default stream). Asynchronous. Runs of one
+ * batch must not overlap on the GPU (they share the counter). */
+zoda_status zoda_batch_run(zoda_batch* batch, void* stream);
+
+/* Total input elements (sum of k * cols) of the batch. */
+uint64_t zoda_batch_elements(const zoda_batch* batch);
+
+void zoda_batch_destroy(zoda_batch* batch);
+
 /* ======================================================================
  * Part 3: a transform for callers that cannot allocate device memory
  * ====================================================================== */

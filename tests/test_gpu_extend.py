@@ -46,7 +46,7 @@ def tile_cols(side: int) -> int:
 
 
 SIDES = [1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096]
-IMPLS = [(s, 1) for s in SIDES] + [(s, 2) for s in SIDES if s >= 128]
+IMPLS = [(s, 1) for s in SIDES] + [(s, 2) for s in SIDES if s >= 32]
 
 
 @pytest.mark.parametrize("side,impl", IMPLS, ids=[f"side{s}-{'direct' if i == 1 else 'tma'}" for s, i in IMPLS])

@@ -201,7 +201,7 @@ zoda_status zoda_ctx_create(int device, zoda_ctx** out) {
     }
     {
         std::vector<Tw> side;
-        for (int ls = 7; ls <= 12; ls++) build_side_tables(ls, side, c->tables.side_off[ls]);
+        for (int ls = 5; ls <= 12; ls++) build_side_tables(ls, side, c->tables.side_off[ls]);
         if ((e = cudaMalloc(&c->tables.side, side.size() * sizeof(Tw))) != cudaSuccess ||
             (e = cudaMemcpy(c->tables.side, side.data(), side.size() * sizeof(Tw), cudaMemcpyHostToDevice)) !=
                 cudaSuccess) {

@@ -1,10 +1,7 @@
 // Instantiations and launchers of the fused extension kernels (extend.cuh,
 // extend_tma.cuh).
-#include <cudaTypedefs.h>
-
 #include "extend.cuh"
-#include "extend_tma.cuh"
-#include "internal.hpp"
+#include "tma_host.hpp"
 
 namespace zb {
 
@@ -17,42 +14,6 @@ __global__ void k_extend_side1(const uint32_t* __restrict__ in, uint32_t* __rest
         st_v4(out + c, x);
         st_v4(out + cols + c, x);
     }
-}
-
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-    });
-    return fn;
-}
-
-// 2-D u32 tensor map: `rows` rows of `cols` elements, rows `row_bytes` apart,
-// boxes of box_r rows x box_c columns, no swizzle, zero fill out of bounds.
-zoda_status make_map(CUtensorMap* m, const void* base, uint64_t cols, uint64_t rows, uint64_t row_bytes,
-                     uint32_t box_c, uint32_t box_r, CUtensorMapSwizzle swz = CU_TENSOR_MAP_SWIZZLE_NONE) {
-    auto fn = encode_fn();
-    if (!fn) {
-        set_last_error_text("cuTensorMapEncodeTiled unavailable");
-        return ZODA_ERR_CUDA;
-    }
-    const cuuint64_t dims[2] = {cols, rows};
-    const cuuint64_t strides[1] = {row_bytes};
-    const cuuint32_t box[2] = {box_c, box_r};
-    const cuuint32_t estr[2] = {1, 1};
-    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, const_cast<void*>(base), dims, strides, box, estr,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) {
-        set_last_error_text("cuTensorMapEncodeTiled failed with CUresult " + std::to_string((int)r));
-        return ZODA_ERR_CUDA;
-    }
-    return ZODA_OK;
 }
 
 template <int LOG_S>
@@ -73,22 +34,10 @@ zoda_status launch_tma_t(const zoda_ctx* ctx, const uint32_t* in, uint32_t* out,
     const uint64_t ntiles = (cols + TP::C - 1) / TP::C;
     if (ntiles == 0) return ZODA_OK;
     CUtensorMap m_in, m_even;
-    const CUtensorMapSwizzle swz = TP::SWZ_MASK == 7   ? CU_TENSOR_MAP_SWIZZLE_128B
-                                   : TP::SWZ_MASK == 3 ? CU_TENSOR_MAP_SWIZZLE_64B
-                                   : TP::SWZ_MASK == 1 ? CU_TENSOR_MAP_SWIZZLE_32B
-                                                       : CU_TENSOR_MAP_SWIZZLE_NONE;
-    zoda_status s = make_map(&m_in, in, cols, TP::S, cols * 4, TP::C, TP::BOX_R, swz);
+    zoda_status s = make_tile_maps<TP>(&m_in, &m_even, in, out, cols);
     if (s != ZODA_OK) return s;
-    if ((s = make_map(&m_even, out, cols, TP::S, cols * 8, TP::C, TP::BOX_R, swz)) != ZODA_OK) return s;
     const uint64_t grid = ntiles < (uint64_t)ctx->sm_count ? ntiles : (uint64_t)ctx->sm_count;
-    SideTables tb;
-    const size_t* off = ctx->tables.side_off[LOG_S];
-    const uint2* base = reinterpret_cast<const uint2*>(ctx->tables.side);
-    tb.intt[0] = base + off[0];
-    tb.intt[1] = base + off[1];
-    tb.ntt0 = base + off[2];
-    tb.ntt[0] = nullptr;  // NTT level 0 uses ntt0
-    tb.ntt[1] = base + off[3];
+    const SideTables tb = side_tables(ctx, LOG_S);
     k_extend_tma<LOG_S><<<(unsigned)grid, 512, TP::SMEM, st>>>(m_in, m_even, out, cols, ntiles, tb, ctx->d_err);
     ZB_CUDA(cudaGetLastError());
     return ZODA_OK;
@@ -99,7 +48,7 @@ zoda_status set_attr_t() {
     using PL = ExtPlan<LOG_S>;
     if (PL::SMEM > 0)
         ZB_CUDA(cudaFuncSetAttribute(k_extend<LOG_S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PL::SMEM));
-    if constexpr (LOG_S >= 7)
+    if constexpr (LOG_S >= 5)
         ZB_CUDA(cudaFuncSetAttribute(k_extend_tma<LOG_S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)TPlan<LOG_S>::SMEM));
     return ZODA_OK;
@@ -122,9 +71,11 @@ zoda_status launch_extend(const zoda_ctx* ctx, int log_s, const uint32_t* in, ui
     // 8-column tiles split 32-byte sectors between the two warp-groups, and the
     // direct-load kernel is faster.
     const bool tma = (impl == 2) || (impl == 0 && log_s >= 7 && log_s <= 11);
-    if (impl == 2 && (log_s < 7 || log_s > 12)) return ZODA_ERR_UNSUPPORTED;
+    if (impl == 2 && (log_s < 5 || log_s > 12)) return ZODA_ERR_UNSUPPORTED;
     if (tma) {
         switch (log_s) {
+            case 5: return launch_tma_t<5>(ctx, in, out, cols, st);
+            case 6: return launch_tma_t<6>(ctx, in, out, cols, st);
             case 7: return launch_tma_t<7>(ctx, in, out, cols, st);
             case 8: return launch_tma_t<8>(ctx, in, out, cols, st);
             case 9: return launch_tma_t<9>(ctx, in, out, cols, st);

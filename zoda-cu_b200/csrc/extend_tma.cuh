@@ -1,4 +1,5 @@
-// Fused extension, TMA-staged variant for sides 128..4096.
+// Fused extension, TMA-staged variant for sides 32..4096, one square per launch
+// or many squares of mixed sides in one persistent launch.
 //
 // Same math and level structure as extend.cuh (INTT DIF levels, twist, NTT DIF
 // levels in mirrored order), organised for latency hiding:
@@ -108,12 +109,17 @@ struct TPlan {
     static constexpr int S = PL::S, C = PL::C, Q4 = PL::Q4, TPQ = PL::TPQ, EPT = PL::EPT;
     static constexpr int NLEV = PL::NLEV;
     static constexpr int GQ = Q4 / 2;  // quads per warp-group
+    // TMA boxes: at most 256 rows x 256 columns; sides below 128 have tiles wider
+    // than 256 columns and stage them as NBOXC column boxes side by side.
     static constexpr int BOX_R = S < 256 ? S : 256;
-    static constexpr int NBOX = S / BOX_R;
+    static constexpr int BOX_C = C < 256 ? C : 256;
+    static constexpr int NBOXR = S / BOX_R, NBOXC = C / BOX_C;
+    static constexpr int NBOX = NBOXR * NBOXC;
     static constexpr uint32_t TILE_BYTES = (uint32_t)S * C * 4;
-    // staging swizzle: rows of C*4 bytes; 0 = none, else the XOR mask on (offset >> 7)
-    static constexpr int ROW_BYTES = C * 4;
+    // staging swizzle: box rows of BOX_C*4 bytes; 0 = none, else the XOR mask on (offset >> 7)
+    static constexpr int ROW_BYTES = BOX_C * 4;
     static constexpr uint32_t SWZ_MASK = ROW_BYTES == 128 ? 7 : ROW_BYTES == 64 ? 3 : ROW_BYTES == 32 ? 1 : 0;
+    static constexpr int QB = BOX_C / 4;  // quads per box row
     using XP = XPad<LOG_S>;
     // Lane map inside a warp: quad ql = lane % GQ, row group t = TW*warp + perm(lane / GQ),
     // perm a bit-linear map (images of the basis vectors) chosen, together with the
@@ -135,8 +141,8 @@ struct TPlan {
     static constexpr size_t OFF_X = TILE_BYTES;
     static constexpr size_t OFF_BAR = (OFF_X + 2 * X_BYTES + 15) / 16 * 16;
     static constexpr size_t SMEM = OFF_BAR + 32;
-    static_assert(LOG_S >= 7 && LOG_S <= 12, "TMA path covers sides 128..4096");
-    static_assert(C <= 256 && GQ >= 1, "box inner dimension");
+    static_assert(LOG_S >= 5 && LOG_S <= 12, "TMA path covers sides 32..4096");
+    static_assert(GQ >= 1, "two warp-groups");
     static_assert(NLEV >= 2, "at least one exchange");
     static_assert(SMEM <= 232448, "shared memory budget");
     static_assert(SWZ_MASK == 0 || (S / 16) * ROW_BYTES % (128 * (SWZ_MASK + 1)) == 0,
@@ -150,12 +156,17 @@ struct TPlan {
         return slot * GQ + XP::PW1 * (slot >> XP::PS1) + (XP::PW2 ? XP::PW2 * (slot >> XP::PS2) : 0);
     }
     __device__ static __forceinline__ uint32_t xword(uint32_t slot, int ql) { return xoff(slot) + (uint32_t)ql; }
-    // staging byte offset of (row, quad)
+    // staging byte offset of (row, quad): column box bc sits at bc * S box rows
     __device__ static __forceinline__ uint32_t stage_off(uint32_t row, int q) {
-        const uint32_t o = row * ROW_BYTES + 16u * (uint32_t)q;
+        const uint32_t bc = (uint32_t)q / QB, qi = (uint32_t)q % QB;
+        const uint32_t o = (bc * S + row) * ROW_BYTES + 16u * qi;
         if constexpr (SWZ_MASK) return o ^ (((o >> 7) & SWZ_MASK) << 4);
         return o;
     }
+    // TMA box b = bc * NBOXR + br: smem element offset and global (x, y) in a tile
+    __device__ static __forceinline__ uint32_t box_smem(int b) { return (uint32_t)b * BOX_R * BOX_C; }
+    __device__ static __forceinline__ int box_x(uint64_t tile, int b) { return (int)(tile * C) + (b / NBOXR) * BOX_C; }
+    __device__ static __forceinline__ int box_y(int b) { return (b % NBOXR) * BOX_R; }
 };
 
 // Per-side twiddle tables in HBM (read through L1), laid out [k2][index] so a
@@ -332,6 +343,103 @@ __device__ __forceinline__ void ntt_from(V4* v, uint2* xg, int t, int ql, int ba
     }
 }
 
+// ---- per-tile pieces shared by the single-square and the batched kernels -------
+
+// Thread coordinates inside its warp-group (see the lane map in TPlan).
+template <class TP>
+struct Coords {
+    int ql, t, q;
+    __device__ __forceinline__ Coords(int ltid, int grp) {
+        const int lane = ltid & 31, wg = ltid >> 5;
+        ql = TP::GQ < 32 ? lane % TP::GQ : ltid % TP::GQ;
+        t = TP::GQ < 32 ? wg * TP::TW + TP::lane_t(lane / TP::GQ) : ltid / TP::GQ;
+        q = grp * TP::GQ + ql;
+    }
+};
+
+template <class TP>
+__device__ __forceinline__ void tma_load_tile(uint32_t* stage, const CUtensorMap* map, uint64_t tile,
+                                              uint64_t* full) {
+    mbar_expect_tx(full, TP::TILE_BYTES);
+#pragma unroll
+    for (int b = 0; b < TP::NBOX; b++)
+        tma_load_2d(stage + TP::box_smem(b), map, TP::box_x(tile, b), TP::box_y(b), full);
+}
+template <class TP>
+__device__ __forceinline__ void tma_store_even(const uint32_t* stage, const CUtensorMap* map, uint64_t tile) {
+#pragma unroll
+    for (int b = 0; b < TP::NBOX; b++) tma_store_2d(map, TP::box_x(tile, b), TP::box_y(b), stage + TP::box_smem(b));
+    bulk_commit();
+}
+
+// INTT level 0 gathers rows t + L0*j of the thread's quad from staging.
+template <class TP>
+__device__ __forceinline__ void stage_read(V4* v, const unsigned char* smem, const Coords<TP>& c) {
+    constexpr int R0 = 1 << TP::lr(0);
+    constexpr int L0 = TP::S / R0;
+    const unsigned char* sb = smem + TP::stage_off((uint32_t)c.t, c.q);
+#pragma unroll
+    for (int j = 0; j < R0; j++) {
+        const uint4 u = *reinterpret_cast<const uint4*>(sb + (size_t)j * L0 * TP::ROW_BYTES);
+        v[j] = V4{{u.x, u.y, u.z, u.w}};
+    }
+}
+
+// Everything after the tile is in registers: INTT, twist, NTT, odd-row stores.
+// With stagger_pending set, group 0 releases group 1 (named barrier 3) from the
+// middle of the tile.
+template <class TP>
+__device__ __forceinline__ void tile_compute(V4* v, uint2* xg, const Coords<TP>& c, int bar, const SideTables& tb,
+                                             uint32_t* __restrict__ out, uint64_t cols, uint64_t col, bool active,
+                                             bool& stagger_pending) {
+    const int t = c.t, ql = c.ql;
+    // ---- INTT levels 0 .. NLEV-2
+    intt_upto_last<TP, 0>(v, xg, t, ql, bar, tb);
+    if (stagger_pending) {
+        asm volatile("bar.arrive 3, 512;" ::: "memory");
+        stagger_pending = false;
+    }
+    {
+        // ---- INTT last level (L = 1). Its outputs need the twist g^c / S with
+        // c = c0 + k2*S/R; g^(k2*S/R) = omega_2R^k2 is an immediate folded into the
+        // last butterfly stage, and g^c0 / S is folded into NTT level 0's table.
+        constexpr int LR = TP::lr(TP::NLEV - 1);
+        constexpr int R = 1 << LR;
+        constexpr int G = TP::EPT / R;
+        constexpr int NB = TP::S / R;  // INTT last-level blocks
+        constexpr int SH = TP::LOG_S - LR;
+        using LV = LvlGeom<TP, LR, TP::pre(TP::NLEV - 1)>;
+        using Rd = LvlGeom<TP, TP::nlr(1), TP::npre(1)>;
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            dft_dif_twout<LR, true, true>(v + g * R, ConstTw<LR + 1, false>{});
+            // NTT level 0 wants coefficient c0 + (S/R)*j in register j
+            V4 y[R];
+#pragma unroll
+            for (int j = 0; j < R; j++) y[j] = v[g * R + bitrev(j, LR)];
+#pragma unroll
+            for (int j = 0; j < R; j++) v[g * R + j] = y[j];
+            // ---- NTT level 0: radix R over stride S/R, then g^c0/S * omega_S^(c0*k2)
+            const TabTw<NB> twf{tb.ntt0 + LV::gid(g, t)};
+            dft_dif_twout<LR, false, false>(v + g * R, twf);
+        }
+        exchange<TP, R, SH, Rd::R, Rd::LOGL>(
+            v, xg, ql, bar, [&](int g) { return digit_rev<typename TP::PL, false>(LV::gid(g, t) << LR); },
+            [&](int g) { return Rd::base(Rd::gid(g, t)); });
+    }
+    // ---- NTT levels 1 .. NLEV-1, the last one stores the odd rows
+    ntt_from<TP, 1>(v, xg, t, ql, bar, tb, out, cols, col, active);
+}
+
+// Re-derive a value from an opaque copy so the compiler rebuilds per-tile
+// addresses inside the loop instead of keeping them all live across it.
+__device__ __forceinline__ int opaque(int x) {
+    int y;
+    asm volatile("mov.u32 %0, %1;" : "=r"(y) : "r"(x));
+    return y;
+}
+
+// ---- one square ------------------------------------------------------------------
 template <int LOG_S>
 __global__ void __launch_bounds__(512, 1)
     k_extend_tma(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_even,
@@ -355,12 +463,7 @@ __global__ void __launch_bounds__(512, 1)
     }
     __syncthreads();
     uint64_t tile = blockIdx.x;
-    if (producer && tile < ntiles) {
-        mbar_expect_tx(full, TP::TILE_BYTES);
-#pragma unroll
-        for (int b = 0; b < TP::NBOX; b++)
-            tma_load_2d(stage + (size_t)b * TP::BOX_R * TP::C, &tm_in, (int)(tile * TP::C), b * TP::BOX_R, full);
-    }
+    if (producer && tile < ntiles) tma_load_tile<TP>(stage, &tm_in, tile, full);
     // Group 1 starts half a tile after group 0 so the two groups' barriers and
     // butterfly phases interleave; group 0 signals from the middle of its first tile.
     if (grp == 1 && tile < ntiles) asm volatile("bar.sync 3, 512;" ::: "memory");
@@ -368,16 +471,8 @@ __global__ void __launch_bounds__(512, 1)
     V4 v[TP::EPT];
     uint32_t parity = 0;
     for (; tile < ntiles; tile += gridDim.x, parity ^= 1) {
-        // Thread coordinates are re-derived each tile from an opaque copy of tid so
-        // the compiler rebuilds the per-pattern smem addresses here instead of
-        // keeping them all live across the loop.
-        int tid_l;
-        asm volatile("mov.u32 %0, %1;" : "=r"(tid_l) : "r"(tid));
-        const int ltid = tid_l & 255;
-        const int lane = ltid & 31, wg = ltid >> 5;
-        const int ql = TP::GQ < 32 ? lane % TP::GQ : ltid % TP::GQ;
-        const int t = TP::GQ < 32 ? wg * TP::TW + TP::lane_t(lane / TP::GQ) : ltid / TP::GQ;
-        const int q = grp * TP::GQ + ql;
+        const int tid_l = opaque(tid);
+        const Coords<TP> c(tid_l & 255, grp);
         uint2* xg = reinterpret_cast<uint2*>(smem + TP::OFF_X + (tid_l >> 8) * TP::X_BYTES);
         const bool ok = mbar_wait_bounded(full, parity);
         if (group_vote_or(bar, !ok)) {
@@ -386,24 +481,10 @@ __global__ void __launch_bounds__(512, 1)
             if (producer) bulk_wait0();
             return;
         }
-        if (producer) {  // even output rows = the input tile, straight from staging
-#pragma unroll
-            for (int b = 0; b < TP::NBOX; b++)
-                tma_store_2d(&tm_even, (int)(tile * TP::C), b * TP::BOX_R, stage + (size_t)b * TP::BOX_R * TP::C);
-            bulk_commit();
-        }
-        const uint64_t col = tile * TP::C + 4 * (uint64_t)q;
+        if (producer) tma_store_even<TP>(stage, &tm_even, tile);  // even output rows = the input tile
+        const uint64_t col = tile * TP::C + 4 * (uint64_t)c.q;
         const bool active = col < cols;
-        {
-            constexpr int R0 = 1 << TP::lr(0);
-            constexpr int L0 = TP::S / R0;
-            const unsigned char* sb = smem + TP::stage_off((uint32_t)t, q);
-#pragma unroll
-            for (int j = 0; j < R0; j++) {
-                const uint4 u = *reinterpret_cast<const uint4*>(sb + (size_t)j * L0 * TP::ROW_BYTES);
-                v[j] = V4{{u.x, u.y, u.z, u.w}};
-            }
-        }
+        stage_read<TP>(v, smem, c);
         group_bar(bar);  // this group has copied the staging buffer out
         if ((tid & 255) == 0) mbar_arrive(empty);
         const uint64_t next = tile + gridDim.x;
@@ -411,53 +492,159 @@ __global__ void __launch_bounds__(512, 1)
             const bool e_ok = mbar_wait_bounded(empty, parity);  // the other group is done too
             bulk_wait_read0();  // the even-row store has finished reading staging
             fence_proxy_async();
-            if (e_ok) {
-                mbar_expect_tx(full, TP::TILE_BYTES);
-#pragma unroll
-                for (int b = 0; b < TP::NBOX; b++)
-                    tma_load_2d(stage + (size_t)b * TP::BOX_R * TP::C, &tm_in, (int)(next * TP::C),
-                                b * TP::BOX_R, full);
-            } else {
-                atomicOr(err, 2);  // both groups then time out on `full` and leave
-            }
+            if (e_ok) tma_load_tile<TP>(stage, &tm_in, next, full);
+            else atomicOr(err, 2);  // both groups then time out on `full` and leave
         }
+        tile_compute<TP>(v, xg, c, bar, tb, out, cols, col, active, stagger_pending);
+    }
+    if (stagger_pending) asm volatile("bar.arrive 3, 512;" ::: "memory");
+    if (producer) bulk_wait0();
+}
 
-        // ---- INTT levels 0 .. NLEV-2
-        intt_upto_last<TP, 0>(v, xg, t, ql, bar, tb);
-        if (stagger_pending) {
-            asm volatile("bar.arrive 3, 512;" ::: "memory");
-            stagger_pending = false;
+// ---- many squares of mixed sides in one persistent launch ---------------------------
+// Work items are (square, column tile) pairs; squares come sorted by decreasing
+// side, and a global counter deals tiles to CTAs in that order, so big squares
+// start first and small ones fill the tail. The producer thread takes the next
+// item, writes its descriptor next to the staging buffer and starts its TMA
+// load; the consumers read the descriptor once the tile has landed.
+struct BatchSquare {
+    CUtensorMap in_map;    // [k][cols] input, boxes of the side's TPlan
+    CUtensorMap even_map;  // even output rows
+    uint32_t* out;
+    uint64_t cols;
+    uint64_t first;        // global index of the square's first tile
+    uint32_t log_s, ntiles;
+    uint32_t pad_[8];
+};
+static_assert(sizeof(BatchSquare) % 64 == 0, "tensor maps stay 64-byte aligned");
+
+constexpr int BATCH_MIN_LOG = 5, BATCH_MAX_LOG = 11;
+constexpr size_t cmax(size_t a, size_t b) { return a > b ? a : b; }
+template <int L, int H>
+struct BatchLayout {
+    static constexpr size_t X = cmax(TPlan<L>::X_BYTES, BatchLayout<L + 1, H>::X);
+};
+template <int H>
+struct BatchLayout<H, H> {
+    static constexpr size_t X = TPlan<H>::X_BYTES;
+};
+constexpr size_t BATCH_X_BYTES = BatchLayout<BATCH_MIN_LOG, BATCH_MAX_LOG>::X;
+constexpr size_t BATCH_OFF_X = 128 * 1024;
+constexpr size_t BATCH_OFF_BAR = (BATCH_OFF_X + 2 * BATCH_X_BYTES + 15) / 16 * 16;
+constexpr size_t BATCH_SMEM = BATCH_OFF_BAR + 64;
+static_assert(BATCH_SMEM <= 232448, "shared memory budget");
+
+struct BatchSlot {  // descriptor of the tile in staging, written by the producer
+    uint32_t sq;     // square index, or BATCH_END when the queue is drained
+    uint32_t log_s;
+    uint64_t tile;
+};
+constexpr uint32_t BATCH_END = 0xFFFFFFFFu;
+
+#define ZB_BATCH_SWITCH(LS, CALL) \
+    switch (LS) {                 \
+        case 5: CALL(5); break;   \
+        case 6: CALL(6); break;   \
+        case 7: CALL(7); break;   \
+        case 8: CALL(8); break;   \
+        case 9: CALL(9); break;   \
+        case 10: CALL(10); break; \
+        default: CALL(11); break; \
+    }
+
+// sq[0..nsq) sorted by first; total_tiles = sum of ntiles; *counter = 0 at launch.
+// (A template only so that the translation units that include this header but
+// never launch it do not compile it.)
+template <int UNUSED = 0>
+__global__ void __launch_bounds__(512, 1)
+    k_extend_batch(const BatchSquare* __restrict__ sq, uint32_t nsq, uint64_t total_tiles,
+                   unsigned long long* __restrict__ counter, const SideTables* __restrict__ tables,
+                   int* __restrict__ err) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    uint32_t* stage = reinterpret_cast<uint32_t*>(smem);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + BATCH_OFF_BAR);
+    uint64_t* empty = full + 1;
+    BatchSlot* slot = reinterpret_cast<BatchSlot*>(smem + BATCH_OFF_BAR + 16);
+    uint32_t* sq_hint = reinterpret_cast<uint32_t*>(smem + BATCH_OFF_BAR + 32);
+    const int tid = threadIdx.x;
+    const int grp = tid >> 8;
+    const int bar = 1 + grp;
+    const bool producer = tid == 256;
+    if (tid == 0) {
+        mbar_init(full, 1);
+        mbar_init(empty, 2);
+        fence_mbar_init();
+        *sq_hint = 0;
+    }
+    __syncthreads();
+    // producer: take the next tile from the queue and start its load
+    auto fetch = [&]() {
+        const unsigned long long g = atomicAdd(counter, 1ull);
+        BatchSlot s{BATCH_END, 0, 0};
+        if (g < total_tiles) {
+            uint32_t i = *sq_hint;  // a CTA's items come in increasing order: short scans
+            while (i + 1 < nsq && sq[i + 1].first <= g) i++;
+            while (i > 0 && sq[i].first > g) i--;
+            *sq_hint = i;
+            s.sq = i;
+            s.log_s = sq[i].log_s;
+            s.tile = g - sq[i].first;
         }
-        {
-            // ---- INTT last level (L = 1). Its outputs need the twist g^c / S with
-            // c = c0 + k2*S/R; g^(k2*S/R) = omega_2R^k2 is an immediate folded into the
-            // last butterfly stage, and g^c0 / S is folded into NTT level 0's table.
-            constexpr int LR = TP::lr(TP::NLEV - 1);
-            constexpr int R = 1 << LR;
-            constexpr int G = TP::EPT / R;
-            constexpr int NB = TP::S / R;  // INTT last-level blocks
-            constexpr int SH = TP::LOG_S - LR;
-            using LV = LvlGeom<TP, LR, TP::pre(TP::NLEV - 1)>;
-            using Rd = LvlGeom<TP, TP::nlr(1), TP::npre(1)>;
-#pragma unroll
-            for (int g = 0; g < G; g++) {
-                dft_dif_twout<LR, true, true>(v + g * R, ConstTw<LR + 1, false>{});
-                // NTT level 0 wants coefficient c0 + (S/R)*j in register j
-                V4 y[R];
-#pragma unroll
-                for (int j = 0; j < R; j++) y[j] = v[g * R + bitrev(j, LR)];
-#pragma unroll
-                for (int j = 0; j < R; j++) v[g * R + j] = y[j];
-                // ---- NTT level 0: radix R over stride S/R, then g^c0/S * omega_S^(c0*k2)
-                const TabTw<NB> twf{tb.ntt0 + LV::gid(g, t)};
-                dft_dif_twout<LR, false, false>(v + g * R, twf);
-            }
-            exchange<TP, R, SH, Rd::R, Rd::LOGL>(
-                v, xg, ql, bar, [&](int g) { return digit_rev<typename TP::PL, false>(LV::gid(g, t) << LR); },
-                [&](int g) { return Rd::base(Rd::gid(g, t)); });
+        *slot = s;
+        if (s.sq == BATCH_END) {
+            mbar_arrive(full);  // completes the phase with no bytes: consumers see the end mark
+        } else {
+            const BatchSquare& b = sq[s.sq];
+#define ZB_LOAD(L) tma_load_tile<TPlan<L>>(stage, &b.in_map, s.tile, full)
+            ZB_BATCH_SWITCH(s.log_s, ZB_LOAD)
+#undef ZB_LOAD
         }
-        // ---- NTT levels 1 .. NLEV-1, the last one stores the odd rows
-        ntt_from<TP, 1>(v, xg, t, ql, bar, tb, out, cols, col, active);
+    };
+    if (producer) fetch();
+    if (grp == 1) asm volatile("bar.sync 3, 512;" ::: "memory");
+    bool stagger_pending = grp == 0;
+    V4 v[16];
+    uint32_t parity = 0;
+    for (;; parity ^= 1) {
+        const int tid_l = opaque(tid);
+        const bool ok = mbar_wait_bounded(full, parity);
+        if (group_vote_or(bar, !ok)) {
+            if ((tid & 255) == 0) atomicOr(err, 1);
+            break;
+        }
+        const BatchSlot s = *slot;
+        if (s.sq == BATCH_END) break;
+        const BatchSquare& b = sq[s.sq];
+        if (producer) {
+#define ZB_STORE(L) tma_store_even<TPlan<L>>(stage, &b.even_map, s.tile)
+            ZB_BATCH_SWITCH(s.log_s, ZB_STORE)
+#undef ZB_STORE
+        }
+        const SideTables& tb = tables[s.log_s];
+        uint32_t* const out = b.out;
+        const uint64_t cols = b.cols;
+        // consumers copy the tile out (arriving on `empty`), then the producer
+        // refills staging while everybody computes
+#define ZB_TILE(L)                                                                               \
+    {                                                                                            \
+        using TP = TPlan<L>;                                                                     \
+        const Coords<TP> c(tid_l & 255, grp);                                                    \
+        uint2* xg = reinterpret_cast<uint2*>(smem + BATCH_OFF_X + (tid_l >> 8) * BATCH_X_BYTES); \
+        stage_read<TP>(v, smem, c);                                                              \
+        group_bar(bar);                                                                          \
+        if ((tid & 255) == 0) mbar_arrive(empty);                                                \
+        if (producer) {                                                                          \
+            const bool e_ok = mbar_wait_bounded(empty, parity);                                  \
+            bulk_wait_read0();                                                                   \
+            fence_proxy_async();                                                                 \
+            if (e_ok) fetch();                                                                   \
+            else atomicOr(err, 2);                                                               \
+        }                                                                                        \
+        const uint64_t col = s.tile * TP::C + 4 * (uint64_t)c.q;                                 \
+        tile_compute<TP>(v, xg, c, bar, tb, out, cols, col, col < cols, stagger_pending);        \
+    }
+        ZB_BATCH_SWITCH(s.log_s, ZB_TILE)
+#undef ZB_TILE
     }
     if (stagger_pending) asm volatile("bar.arrive 3, 512;" ::: "memory");
     if (producer) bulk_wait0();

@@ -38,7 +38,7 @@ struct DevBuf {
 struct Tables {
     Tw* tw = nullptr;
     Tw* twist = nullptr;
-    // per-side level tables of the TMA-staged kernel (log2 side 7..12), one buffer
+    // per-side level tables of the TMA-staged kernels (log2 side 5..12), one buffer
     Tw* side = nullptr;
     size_t side_off[13][5] = {};  // [log_s][intt0, intt1, ntt0, ntt1, end] entry offsets
 };

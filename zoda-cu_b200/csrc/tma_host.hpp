@@ -1,0 +1,75 @@
+// Host-side helpers of the TMA-staged kernels: tensor maps and per-side tables.
+#pragma once
+#include <cudaTypedefs.h>
+
+#include <mutex>
+#include <string>
+
+#include "extend_tma.cuh"
+#include "internal.hpp"
+
+namespace zb {
+
+inline PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    });
+    return fn;
+}
+
+// 2-D u32 tensor map: `rows` rows of `cols` elements, rows `row_bytes` apart,
+// boxes of box_r rows x box_c columns, zero fill out of bounds.
+inline zoda_status make_map(CUtensorMap* m, const void* base, uint64_t cols, uint64_t rows, uint64_t row_bytes,
+                            uint32_t box_c, uint32_t box_r, CUtensorMapSwizzle swz = CU_TENSOR_MAP_SWIZZLE_NONE) {
+    auto fn = encode_fn();
+    if (!fn) {
+        set_last_error_text("cuTensorMapEncodeTiled unavailable");
+        return ZODA_ERR_CUDA;
+    }
+    const cuuint64_t dims[2] = {cols, rows};
+    const cuuint64_t strides[1] = {row_bytes};
+    const cuuint32_t box[2] = {box_c, box_r};
+    const cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, const_cast<void*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_last_error_text("cuTensorMapEncodeTiled failed with CUresult " + std::to_string((int)r));
+        return ZODA_ERR_CUDA;
+    }
+    return ZODA_OK;
+}
+
+// The input map and the even-output-row map of one square for side plan TP.
+template <class TP>
+zoda_status make_tile_maps(CUtensorMap* m_in, CUtensorMap* m_even, const uint32_t* in, uint32_t* out,
+                           uint64_t cols) {
+    const CUtensorMapSwizzle swz = TP::SWZ_MASK == 7   ? CU_TENSOR_MAP_SWIZZLE_128B
+                                   : TP::SWZ_MASK == 3 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                   : TP::SWZ_MASK == 1 ? CU_TENSOR_MAP_SWIZZLE_32B
+                                                       : CU_TENSOR_MAP_SWIZZLE_NONE;
+    zoda_status s = make_map(m_in, in, cols, TP::S, cols * 4, TP::BOX_C, TP::BOX_R, swz);
+    if (s != ZODA_OK) return s;
+    return make_map(m_even, out, cols, TP::S, cols * 8, TP::BOX_C, TP::BOX_R, swz);
+}
+
+// Device pointers of the side's level tables (built in zoda_ctx_create).
+inline SideTables side_tables(const zoda_ctx* ctx, int log_s) {
+    SideTables tb;
+    const size_t* off = ctx->tables.side_off[log_s];
+    const uint2* base = reinterpret_cast<const uint2*>(ctx->tables.side);
+    tb.intt[0] = base + off[0];
+    tb.intt[1] = base + off[1];
+    tb.ntt0 = base + off[2];
+    tb.ntt[0] = nullptr;  // NTT level 0 reads ntt0
+    tb.ntt[1] = base + off[3];
+    return tb;
+}
+
+}  // namespace zb

@@ -32,7 +32,8 @@ EXPORTS = [
     "cuda_ntt", "cuda_intt", "cuda_host_alloc", "cuda_host_free",
     "zoda_status_string", "zoda_last_error", "zoda_ctx_create", "zoda_ctx_destroy", "zoda_max_side",
     "zoda_extend_device", "zoda_extend_host", "zoda_ctx_set_impl", "zoda_ctx_check",
-    "zoda_ntt_device_noalloc",
+    "zoda_ntt_device_noalloc", "zoda_batch_create", "zoda_batch_run", "zoda_batch_elements",
+    "zoda_batch_destroy",
 ]
 
 _lib = None
@@ -42,6 +43,11 @@ class ZodaError(RuntimeError):
     def __init__(self, status: int, where: str, detail: str = ""):
         self.status = status
         super().__init__(f"{where}: {STATUS.get(status, status)}" + (f" ({detail})" if detail else ""))
+
+
+class ZodaSquare(ctypes.Structure):
+    _fields_ = [("d_in", ctypes.c_void_p), ("d_out", ctypes.c_void_p), ("k", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("cols", ctypes.c_uint64)]
 
 
 class ZodaTiming(ctypes.Structure):
@@ -83,6 +89,14 @@ def load(path: str = LIB_PATH):
     L.zoda_ctx_set_impl.argtypes = [vp, ctypes.c_int]
     L.zoda_ctx_check.restype = ctypes.c_int
     L.zoda_ctx_check.argtypes = [vp]
+    L.zoda_batch_create.restype = ctypes.c_int
+    L.zoda_batch_create.argtypes = [vp, ctypes.POINTER(ZodaSquare), ctypes.c_uint32, ctypes.POINTER(vp)]
+    L.zoda_batch_run.restype = ctypes.c_int
+    L.zoda_batch_run.argtypes = [vp, vp]
+    L.zoda_batch_elements.restype = ctypes.c_uint64
+    L.zoda_batch_elements.argtypes = [vp]
+    L.zoda_batch_destroy.restype = None
+    L.zoda_batch_destroy.argtypes = [vp]
     L.zoda_ntt_device_noalloc.restype = ctypes.c_int
     L.zoda_ntt_device_noalloc.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, vp]
     L.zoda_extend_host.restype = ctypes.c_int
@@ -158,6 +172,48 @@ class Context:
         _check(load().zoda_extend_host(self._h, _addr(h_in), _addr(h_out), k, cols, ctypes.byref(t)),
                "zoda_extend_host")
         return t
+
+
+def _stream_handle(stream):
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream()
+    s = stream if isinstance(stream, int) else stream.cuda_stream
+    return s or None
+
+
+class Batch:
+    """Many squares of mixed sides (32..2048) encoded by one persistent,
+    graph-captured launch (zoda_batch_create / zoda_batch_run)."""
+
+    def __init__(self, ctx: Context, squares):
+        """squares: iterable of (d_in, d_out, k, cols) on the context's device."""
+        sq = list(squares)
+        arr = (ZodaSquare * max(1, len(sq)))()
+        for i, (a, b, k, cols) in enumerate(sq):
+            arr[i] = ZodaSquare(_addr(a), _addr(b), k, 0, cols)
+        h = ctypes.c_void_p()
+        _check(load().zoda_batch_create(ctx.handle, arr, len(sq), ctypes.byref(h)), "zoda_batch_create")
+        self._h = h
+        self._keep = sq  # the buffers must outlive the batch
+
+    @property
+    def elements(self) -> int:
+        return int(load().zoda_batch_elements(self._h))
+
+    def run(self, stream=None):
+        _check(load().zoda_batch_run(self._h, _stream_handle(stream)), "zoda_batch_run")
+
+    def close(self):
+        if self._h:
+            load().zoda_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def max_side() -> int:
