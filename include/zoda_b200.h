@@ -171,6 +171,71 @@ uint64_t zoda_batch_elements(const zoda_batch* batch);
 
 void zoda_batch_destroy(zoda_batch* batch);
 
+/* ----------------------------------------------------------------------
+ * Serving loop: squares arrive one by one and are encoded with continuous
+ * batching. No reference counterpart (the reference has no server).
+ *
+ * A native thread owns the GPU side. Every pass it retires finished
+ * launches, then admits waiting requests in arrival order while their
+ * outputs fit in the HBM budget (an output arena allocated once at
+ * creation) and launches them together as one batched kernel on a free
+ * stream. Requests that arrive while others run join the next launch, and
+ * up to `max_inflight` launches overlap on the device.
+ * ---------------------------------------------------------------------- */
+
+typedef struct zoda_server zoda_server;
+
+typedef struct zoda_server_config {
+    uint64_t hbm_budget_bytes; /* output arena size = admission budget; 0 = 64 GiB   */
+    uint32_t max_inflight;     /* launches in flight (streams); 0 = 4                */
+    uint32_t max_batch;        /* squares per launch; 0 = 128                        */
+} zoda_server_config;
+
+typedef struct zoda_request_info {
+    uint32_t* d_out;   /* output [2k][cols], row-major, in the server's arena       */
+    double queue_ms;   /* submit -> launch                                          */
+    double latency_ms; /* submit -> completion observed by the server thread       */
+    int32_t status;    /* zoda_status of the request                                */
+    int32_t reserved;
+} zoda_request_info;
+
+typedef struct zoda_server_stats {
+    uint64_t submitted, completed, cancelled, launches;
+    uint64_t elements;   /* input elements of completed requests */
+    double p50_ms, p99_ms, mean_ms, max_ms; /* latency of completed requests */
+    double first_submit_to_last_done_ms;
+} zoda_server_stats;
+
+/* Creates the server on ctx's device: allocates the output arena and the
+ * per-stream descriptor buffers, starts the thread. ZODA_ERR_NOMEM when the
+ * arena does not fit. */
+zoda_status zoda_server_create(zoda_ctx* ctx, const zoda_server_config* cfg, zoda_server** out);
+
+/* Queues one square: d_in row-major [k][cols] in device memory, k a power of
+ * two in [32, 2048], cols a multiple of 4. d_in must stay valid and unchanged
+ * until the request completes. ZODA_ERR_BUDGET if its output (8*k*cols bytes)
+ * exceeds the whole budget. Returns at once with a ticket. */
+zoda_status zoda_server_submit(zoda_server* srv, const uint32_t* d_in, uint32_t k, uint64_t cols,
+                               uint64_t* ticket);
+
+/* Waits up to timeout_ms (0 = do not wait) for the request; ZODA_ERR_TIMEOUT
+ * if it has not finished. On success info describes it; the output stays in
+ * the arena until zoda_server_release. */
+zoda_status zoda_server_wait(zoda_server* srv, uint64_t ticket, uint32_t timeout_ms, zoda_request_info* info);
+
+/* Returns a finished request's output region to the arena. */
+zoda_status zoda_server_release(zoda_server* srv, uint64_t ticket);
+
+/* Drops a request that has not been launched yet (ZODA_ERR_STATE otherwise);
+ * a later wait reports ZODA_ERR_CANCELLED. */
+zoda_status zoda_server_cancel(zoda_server* srv, uint64_t ticket);
+
+zoda_status zoda_server_get_stats(zoda_server* srv, zoda_server_stats* stats);
+
+/* Stops the thread after in-flight launches finish; queued requests are
+ * cancelled. */
+void zoda_server_destroy(zoda_server* srv);
+
 /* ======================================================================
  * Part 3: a transform for callers that cannot allocate device memory
  * ====================================================================== */

@@ -47,6 +47,42 @@ int log2_side(uint32_t k) {
 }
 
 }  // namespace
+
+zoda_status make_batch_square(const zoda_square& q, BatchSquare* b) {
+    const int ls = log2_side(q.k);
+    if (!q.d_in || !q.d_out || ls < 0 || q.cols % 4 || (((uintptr_t)q.d_in | (uintptr_t)q.d_out) & 15))
+        return ZODA_ERR_ARG;
+    if (ls < BATCH_MIN_LOG || ls > BATCH_MAX_LOG) {
+        set_last_error_text("batched sides are 32 .. 2048");
+        return ZODA_ERR_UNSUPPORTED;
+    }
+    memset(b, 0, sizeof *b);
+    switch (ls) {
+        case 5: return fill_square<5>(b, q);
+        case 6: return fill_square<6>(b, q);
+        case 7: return fill_square<7>(b, q);
+        case 8: return fill_square<8>(b, q);
+        case 9: return fill_square<9>(b, q);
+        case 10: return fill_square<10>(b, q);
+        default: return fill_square<11>(b, q);
+    }
+}
+
+zoda_status launch_batch_kernel(const zoda_ctx* ctx, const BatchSquare* d_sq, uint32_t nsq, uint64_t total_tiles,
+                                unsigned long long* d_counter, const SideTables* d_tables, cudaStream_t st) {
+    if (total_tiles == 0) return ZODA_OK;
+    const uint64_t grid = total_tiles < (uint64_t)ctx->sm_count ? total_tiles : (uint64_t)ctx->sm_count;
+    k_extend_batch<0><<<(unsigned)grid, 512, BATCH_SMEM, st>>>(d_sq, nsq, total_tiles, d_counter, d_tables,
+                                                                ctx->d_err);
+    ZB_CUDA(cudaGetLastError());
+    return ZODA_OK;
+}
+
+zoda_status set_batch_kernel_attributes() {
+    ZB_CUDA(cudaFuncSetAttribute(k_extend_batch<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BATCH_SMEM));
+    return ZODA_OK;
+}
+
 }  // namespace zb
 
 using namespace zb;
@@ -57,34 +93,14 @@ zoda_status zoda_batch_create(zoda_ctx* ctx, const zoda_square* squares, uint32_
     if (!ctx || !out || (n && !squares)) return ZODA_ERR_ARG;
     *out = nullptr;
     std::vector<uint32_t> order(n);
-    for (uint32_t i = 0; i < n; i++) {
-        const zoda_square& q = squares[i];
-        const int ls = log2_side(q.k);
-        if (!q.d_in || !q.d_out || ls < 0 || q.cols % 4 || (((uintptr_t)q.d_in | (uintptr_t)q.d_out) & 15))
-            return ZODA_ERR_ARG;
-        if (ls < BATCH_MIN_LOG || ls > BATCH_MAX_LOG) {
-            set_last_error_text("zoda_batch_create: batch sides are 32 .. 2048");
-            return ZODA_ERR_UNSUPPORTED;
-        }
-        order[i] = i;
-    }
+    for (uint32_t i = 0; i < n; i++) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return squares[a].k > squares[b].k; });
     std::vector<BatchSquare> host(n);
     uint64_t first = 0, elements = 0;
     for (uint32_t j = 0; j < n; j++) {
         const zoda_square& q = squares[order[j]];
         BatchSquare& b = host[j];
-        memset(&b, 0, sizeof b);
-        zoda_status s;
-        switch (log2_side(q.k)) {
-            case 5: s = fill_square<5>(&b, q); break;
-            case 6: s = fill_square<6>(&b, q); break;
-            case 7: s = fill_square<7>(&b, q); break;
-            case 8: s = fill_square<8>(&b, q); break;
-            case 9: s = fill_square<9>(&b, q); break;
-            case 10: s = fill_square<10>(&b, q); break;
-            default: s = fill_square<11>(&b, q); break;
-        }
+        const zoda_status s = make_batch_square(q, &b);
         if (s != ZODA_OK) return s;
         b.first = first;
         first += b.ntiles;
@@ -120,11 +136,7 @@ zoda_status zoda_batch_create(zoda_ctx* ctx, const zoda_square* squares, uint32_
         set_last_error("cudaMemcpy(batch tables)", e);
         return fail(ZODA_ERR_CUDA);
     }
-    if ((e = cudaFuncSetAttribute(k_extend_batch<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BATCH_SMEM)) !=
-        cudaSuccess) {
-        set_last_error("cudaFuncSetAttribute(k_extend_batch)", e);
-        return fail(ZODA_ERR_CUDA);
-    }
+    if ((s = set_batch_kernel_attributes()) != ZODA_OK) return fail(s);
     *out = bt;
     return ZODA_OK;
 }
@@ -139,16 +151,11 @@ zoda_status zoda_batch_run(zoda_batch* bt, void* stream) {
         ZB_CUDA(cudaStreamCreateWithFlags(&bt->cap, cudaStreamNonBlocking));
         ZB_CUDA(cudaStreamBeginCapture(bt->cap, cudaStreamCaptureModeThreadLocal));
         cudaMemsetAsync(bt->counter.p, 0, sizeof(unsigned long long), bt->cap);
-        const uint64_t grid = bt->total_tiles < (uint64_t)ctx->sm_count ? bt->total_tiles : (uint64_t)ctx->sm_count;
-        k_extend_batch<0><<<(unsigned)grid, 512, BATCH_SMEM, bt->cap>>>(
-            (const BatchSquare*)bt->squares.p, bt->nsq, bt->total_tiles, (unsigned long long*)bt->counter.p,
-            (const SideTables*)bt->tables.p, ctx->d_err);
-        const cudaError_t launch_err = cudaGetLastError();
+        const zoda_status ls = launch_batch_kernel(ctx, (const BatchSquare*)bt->squares.p, bt->nsq, bt->total_tiles,
+                                                   (unsigned long long*)bt->counter.p,
+                                                   (const SideTables*)bt->tables.p, bt->cap);
         cudaError_t e = cudaStreamEndCapture(bt->cap, &bt->graph);
-        if (launch_err != cudaSuccess) {
-            set_last_error("k_extend_batch launch", launch_err);
-            return ZODA_ERR_CUDA;
-        }
+        if (ls != ZODA_OK) return ls;
         if (e != cudaSuccess) {
             set_last_error("cudaStreamEndCapture", e);
             return ZODA_ERR_CUDA;

@@ -73,3 +73,14 @@ inline SideTables side_tables(const zoda_ctx* ctx, int log_s) {
 }
 
 }  // namespace zb
+
+namespace zb {
+// Batch building blocks shared by zoda_batch_* and the serving loop (batch.cu).
+// Descriptor of one square; ZODA_ERR_UNSUPPORTED outside sides 32..2048.
+zoda_status make_batch_square(const zoda_square& q, BatchSquare* out);
+// One launch of k_extend_batch over d_sq[0..nsq) (sorted by first), with
+// *d_counter already zero on `st`.
+zoda_status launch_batch_kernel(const zoda_ctx* ctx, const BatchSquare* d_sq, uint32_t nsq, uint64_t total_tiles,
+                                unsigned long long* d_counter, const SideTables* d_tables, cudaStream_t st);
+zoda_status set_batch_kernel_attributes();
+}  // namespace zb

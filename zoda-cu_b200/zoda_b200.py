@@ -33,7 +33,8 @@ EXPORTS = [
     "zoda_status_string", "zoda_last_error", "zoda_ctx_create", "zoda_ctx_destroy", "zoda_max_side",
     "zoda_extend_device", "zoda_extend_host", "zoda_ctx_set_impl", "zoda_ctx_check",
     "zoda_ntt_device_noalloc", "zoda_batch_create", "zoda_batch_run", "zoda_batch_elements",
-    "zoda_batch_destroy",
+    "zoda_batch_destroy", "zoda_server_create", "zoda_server_submit", "zoda_server_wait",
+    "zoda_server_release", "zoda_server_cancel", "zoda_server_get_stats", "zoda_server_destroy",
 ]
 
 _lib = None
@@ -48,6 +49,23 @@ class ZodaError(RuntimeError):
 class ZodaSquare(ctypes.Structure):
     _fields_ = [("d_in", ctypes.c_void_p), ("d_out", ctypes.c_void_p), ("k", ctypes.c_uint32),
                 ("reserved", ctypes.c_uint32), ("cols", ctypes.c_uint64)]
+
+
+class ZodaServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_uint64), ("max_inflight", ctypes.c_uint32),
+                ("max_batch", ctypes.c_uint32)]
+
+
+class ZodaRequestInfo(ctypes.Structure):
+    _fields_ = [("d_out", ctypes.c_void_p), ("queue_ms", ctypes.c_double), ("latency_ms", ctypes.c_double),
+                ("status", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class ZodaServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("cancelled", ctypes.c_uint64),
+                ("launches", ctypes.c_uint64), ("elements", ctypes.c_uint64), ("p50_ms", ctypes.c_double),
+                ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double),
+                ("first_submit_to_last_done_ms", ctypes.c_double)]
 
 
 class ZodaTiming(ctypes.Structure):
@@ -97,6 +115,20 @@ def load(path: str = LIB_PATH):
     L.zoda_batch_elements.argtypes = [vp]
     L.zoda_batch_destroy.restype = None
     L.zoda_batch_destroy.argtypes = [vp]
+    L.zoda_server_create.restype = ctypes.c_int
+    L.zoda_server_create.argtypes = [vp, ctypes.POINTER(ZodaServerConfig), ctypes.POINTER(vp)]
+    L.zoda_server_submit.restype = ctypes.c_int
+    L.zoda_server_submit.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]
+    L.zoda_server_wait.restype = ctypes.c_int
+    L.zoda_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(ZodaRequestInfo)]
+    L.zoda_server_release.restype = ctypes.c_int
+    L.zoda_server_release.argtypes = [vp, ctypes.c_uint64]
+    L.zoda_server_cancel.restype = ctypes.c_int
+    L.zoda_server_cancel.argtypes = [vp, ctypes.c_uint64]
+    L.zoda_server_get_stats.restype = ctypes.c_int
+    L.zoda_server_get_stats.argtypes = [vp, ctypes.POINTER(ZodaServerStats)]
+    L.zoda_server_destroy.restype = None
+    L.zoda_server_destroy.argtypes = [vp]
     L.zoda_ntt_device_noalloc.restype = ctypes.c_int
     L.zoda_ntt_device_noalloc.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, vp]
     L.zoda_extend_host.restype = ctypes.c_int
@@ -207,6 +239,65 @@ class Batch:
     def close(self):
         if self._h:
             load().zoda_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_cudart = None
+
+
+def device_copy(dst, src, nbytes: int):
+    """cudaMemcpy (device to device) between raw addresses or tensors; used to read
+    outputs that live in a server's arena."""
+    global _cudart
+    if _cudart is None:
+        _cudart = ctypes.CDLL("libcudart.so.12")
+        _cudart.cudaMemcpy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+        _cudart.cudaMemcpy.restype = ctypes.c_int
+    err = _cudart.cudaMemcpy(_addr(dst), _addr(src), nbytes, 3)
+    if err != 0:
+        raise RuntimeError(f"cudaMemcpy failed with {err}")
+
+
+class Server:
+    """Serving loop with continuous batching (zoda_server_*): submit squares as they
+    arrive, wait for each, read its output from the server's arena, release it."""
+
+    def __init__(self, ctx: Context, budget_bytes: int = 0, max_inflight: int = 0, max_batch: int = 0):
+        cfg = ZodaServerConfig(budget_bytes, max_inflight, max_batch)
+        h = ctypes.c_void_p()
+        _check(load().zoda_server_create(ctx.handle, ctypes.byref(cfg), ctypes.byref(h)), "zoda_server_create")
+        self._h = h
+
+    def submit(self, d_in, k: int, cols: int) -> int:
+        t = ctypes.c_uint64()
+        _check(load().zoda_server_submit(self._h, _addr(d_in), k, cols, ctypes.byref(t)), "zoda_server_submit")
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = 60000) -> ZodaRequestInfo:
+        info = ZodaRequestInfo()
+        _check(load().zoda_server_wait(self._h, ticket, timeout_ms, ctypes.byref(info)), "zoda_server_wait")
+        return info
+
+    def release(self, ticket: int):
+        _check(load().zoda_server_release(self._h, ticket), "zoda_server_release")
+
+    def cancel(self, ticket: int):
+        _check(load().zoda_server_cancel(self._h, ticket), "zoda_server_cancel")
+
+    def stats(self) -> ZodaServerStats:
+        st = ZodaServerStats()
+        _check(load().zoda_server_get_stats(self._h, ctypes.byref(st)), "zoda_server_get_stats")
+        return st
+
+    def close(self):
+        if self._h:
+            load().zoda_server_destroy(self._h)
             self._h = None
 
     def __del__(self):
