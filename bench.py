@@ -309,6 +309,129 @@ def time_reference_cuda(side: int, iters: int = 2):
             "window": "intt_cuda + ntt_cuda with PCIe (reference's 'GPU xform')"}
 
 
+def log_uniform_sides(n: int, lo: int, hi: int, seed: int):
+    rng = __import__("numpy").random.default_rng(seed)
+    return [1 << int(rng.integers(lo.bit_length() - 1, hi.bit_length())) for _ in range(n)]
+
+
+def time_batched(ctx, n: int) -> dict:
+    """n squares, sides log-uniform over 32..2048 (seed 0), 128 u32 per share: one batched
+    persistent launch (graph replay) against plain calls, one square at a time."""
+    import torch
+    import zoda_b200
+    sides = log_uniform_sides(n, 32, 2048, seed=0)
+    sq = []
+    for s in sides:
+        a = torch.randint(0, P, (s, s * SHARE_U32), dtype=torch.int64, device="cuda").to(torch.int32)
+        sq.append((a, torch.empty((2 * s, s * SHARE_U32), dtype=torch.int32, device="cuda"), s, s * SHARE_U32))
+    payload = sum(payload_bits(s) for s in sides)
+    batch = zoda_b200.Batch(ctx, sq)
+    stream = torch.cuda.current_stream()
+    for _ in range(3):
+        batch.run(stream)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 3
+    ev0.record(stream)
+    for _ in range(reps):
+        batch.run(stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    tb = ev0.elapsed_time(ev1) / reps
+    # plain: one zoda_extend_device call per square, each waited for before the next
+    for a, b, s, c in sq[:4]:
+        ctx.extend(a, b, s, c)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for a, b, s, c in sq:
+        ctx.extend(a, b, s, c)
+        torch.cuda.synchronize()
+    tp = (time.perf_counter() - t0) * 1e3
+    # spot check: the batch and the plain calls wrote the same outputs
+    b_out = sq[-1][1].clone()
+    batch.run(stream)
+    torch.cuda.synchronize()
+    assert torch.equal(b_out, sq[-1][1])
+    batch.close()
+    per_side = {}
+    for s in sorted(set(sides)):
+        per_side[str(s)] = sides.count(s)
+    del sq
+    torch.cuda.empty_cache()
+    return {"squares": n, "sides_drawn": per_side, "payload_gb": round(payload / 8e9, 3),
+            "batched_ms": round(tb, 3), "batched_gbps": round(payload / (tb * 1e-3) / 1e9, 1),
+            "plain_ms": round(tp, 3), "plain_gbps": round(payload / (tp * 1e-3) / 1e9, 1),
+            "speedup": round(tp / tb, 3),
+            "note": "plain = one zoda_extend_device per square, synchronized (one square at a time)"}
+
+
+def time_serving(ctx, rate: float, nreq: int, budget_gib: int = 64) -> dict:
+    """Seeded Poisson arrivals at `rate` squares/s, sides log-uniform over 64..2048,
+    payloads pre-staged in HBM (one input per side), 64 GiB output budget; p50/p99
+    latency and sustained Gb/s, against the same requests as sequential plain calls."""
+    import threading
+    import numpy as np
+    import torch
+    import zoda_b200
+    rng = np.random.default_rng(1)
+    sides = log_uniform_sides(nreq, 64, 2048, seed=1)
+    gaps = rng.exponential(1.0 / rate, nreq)
+    inputs = {s: torch.randint(0, P, (s, s * SHARE_U32), dtype=torch.int64, device="cuda").to(torch.int32)
+              for s in sorted(set(sides))}
+    torch.cuda.synchronize()
+    srv = zoda_b200.Server(ctx, budget_bytes=budget_gib << 30, max_inflight=4, max_batch=128)
+    tickets = [None] * nreq
+    submitted = threading.Event()
+
+    def producer():  # open-loop arrivals: sleep (GIL released) until just before each one
+        t_next = time.perf_counter()
+        for i, s in enumerate(sides):
+            t_next += gaps[i]
+            while True:
+                dt = t_next - time.perf_counter()
+                if dt <= 0:
+                    break
+                time.sleep(dt if dt < 2e-4 else dt - 1e-4)
+            tickets[i] = srv.submit(inputs[s], s, s * SHARE_U32)
+        submitted.set()
+
+    old_switch = sys.getswitchinterval()
+    sys.setswitchinterval(2e-5)  # the submitting and the waiting thread both stay responsive
+    th = threading.Thread(target=producer)
+    t0 = time.perf_counter()
+    th.start()
+    lat = []
+    for i in range(nreq):
+        while tickets[i] is None:
+            time.sleep(0.0001)
+        info = srv.wait(tickets[i])
+        lat.append(info.latency_ms)
+        srv.release(tickets[i])
+    th.join()
+    wall = time.perf_counter() - t0
+    sys.setswitchinterval(old_switch)
+    st = srv.stats()
+    srv.close()
+    payload = sum(payload_bits(s) for s in sides)
+    # the same requests as plain sequential calls
+    outs = {s: torch.empty((2 * s, s * SHARE_U32), dtype=torch.int32, device="cuda") for s in inputs}
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for s in sides:
+        ctx.extend(inputs[s], outs[s], s, s * SHARE_U32)
+        torch.cuda.synchronize()
+    tplain = time.perf_counter() - t1
+    del inputs, outs
+    torch.cuda.empty_cache()
+    lat.sort()
+    return {"requests": nreq, "offered_rate_per_s": rate, "offered_gbps": round(payload / (gaps.sum()) / 1e9, 1),
+            "sustained_gbps": round(payload / (st.first_submit_to_last_done_ms * 1e-3) / 1e9, 1),
+            "p50_ms": round(st.p50_ms, 3), "p99_ms": round(st.p99_ms, 3), "max_ms": round(st.max_ms, 3),
+            "launches": int(st.launches), "wall_s": round(wall, 3),
+            "plain_sequential_gbps": round(payload / tplain / 1e9, 1),
+            "budget_gib": budget_gib, "sides": "log-uniform 64..2048, 128 u32/share, seed 1"}
+
+
 def run_ours(args, world, rank, local):
     import torch
     import zoda_b200
@@ -352,6 +475,9 @@ def run_ours(args, world, rank, local):
         refc = time_reference_cuda(min(side, 1024))
         if refc:
             extra["reference_cuda_kernel"] = refc
+        if not args.no_batch:
+            extra["batched_mixed_squares"] = time_batched(ctx, args.batch_squares)
+            extra["serving"] = time_serving(ctx, args.serve_rate, args.serve_requests)
     if rank == 0:
         cpu = cpu_port_rate(side, args.cpu_budget)
         cpu.pop("seconds", None)
@@ -392,6 +518,10 @@ def main():
     ap.add_argument("--side", type=int, default=1024)
     ap.add_argument("--extra-sides", type=int, nargs="*", default=[2048, 4096])
     ap.add_argument("--no-extra", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched and serving report lines")
+    ap.add_argument("--batch-squares", type=int, default=96)
+    ap.add_argument("--serve-rate", type=float, default=2000.0)
+    ap.add_argument("--serve-requests", type=int, default=1000)
     ap.add_argument("--cpu-budget", type=float, default=10.0, help="seconds of CPU baseline sampling")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps
