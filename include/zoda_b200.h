@@ -236,6 +236,40 @@ zoda_status zoda_server_get_stats(zoda_server* srv, zoda_server_stats* stats);
  * cancelled. */
 void zoda_server_destroy(zoda_server* srv);
 
+/* ----------------------------------------------------------------------
+ * Any shape, and recovery from erasures
+ * ---------------------------------------------------------------------- */
+
+/* Encode of k data rows with n parity rows, as src/benchmarks/utils.rs:100-146
+ * and src/zoda/babybear.rs:137-152 define it: n_k = next_pow2(k) and
+ * n_kn = next_pow2(k + n) (utils.rs:42-48); the k rows, zero-padded to n_k,
+ * are interpolated over n_k points and evaluated at the n_kn points
+ * omega_{n_kn}^j; d_out receives rows j = 0 .. k+n-1 (the encoded_rows of
+ * utils.rs:167-168), row-major [k+n][cols]. d_in is row-major [k][cols].
+ * Limits: next_pow2(k) <= 4096, k + n <= 2^27, cols % 4 == 0, 16-byte aligned
+ * buffers that do not overlap. n == k with k a power of two is exactly
+ * zoda_extend_device; every other shape runs one interpolation and one
+ * evaluation per coset on the general column transform, in column chunks
+ * whose scratch (<= 256 MiB) the context keeps. Asynchronous on `stream`. */
+zoda_status zoda_encode_device(zoda_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t k, uint32_t n,
+                               uint64_t cols, void* stream);
+
+/* k-of-2k erasure decoder. No counterpart in the reference, whose tests only
+ * re-encode and RLC-check (utils.rs:186-272); this is the recovery a sampling
+ * light node or a repairing full node runs.
+ * d_code is the [2k][cols] extension (rows in natural order, as
+ * zoda_extend_device writes them); only the rows listed in known_rows[0 ..
+ * nknown) are read, the others may hold anything. At least k distinct rows
+ * must be known. d_data receives the original [k][cols] data. k is a power of
+ * two <= 2048. When every even row is known the data is copied out; otherwise
+ * the call runs four column transforms over 2k points (see general.cu) with
+ * the context's scratch (<= 512 MiB). If `mismatch` is not NULL the call also
+ * checks that the known rows are one codeword, stores the number of
+ * inconsistent coefficients there (0 = consistent) and synchronizes `stream`;
+ * otherwise it is asynchronous on `stream`. */
+zoda_status zoda_recover_device(zoda_ctx* ctx, const uint32_t* d_code, const uint32_t* known_rows, uint32_t nknown,
+                                uint32_t k, uint64_t cols, uint32_t* d_data, uint64_t* mismatch, void* stream);
+
 /* ======================================================================
  * Part 3: a transform for callers that cannot allocate device memory
  * ====================================================================== */

@@ -1,0 +1,83 @@
+// General column transform on row-major matrices, the building block of the
+// encode for any (k, n) and of the erasure decoder.
+//
+// For every column c in [0, cols) and output row r < out_rows:
+//   out[r * out_pitch + c] = post(r) * sum_{i < N} pre(i) * in[i * in_pitch + c] * omega_N^(+-i*r)
+// with N = 2^LOG_N, in[i] = 0 for i >= in_rows (those rows are never read),
+// pre(i) = 1 when no pre table is given, post(r) = post[r] when a post table is
+// given and `scale` otherwise; rows whose pre-factor is 0 are not read. Tables
+// hold (w, floor(w * 2^32 / p)) pairs, the Shoup form every product here uses.
+//
+// Same register-resident DIF levels as the extension kernels (extend.cuh): the
+// thread's quad of 4 adjacent columns, radix-16 levels exchanged through shared
+// memory, natural-order output by digit reversal. Row pre-factors are applied
+// as the rows are loaded, so a pointwise scaling never costs its own HBM pass.
+#pragma once
+#include "extend.cuh"
+
+namespace zb {
+
+struct ColTx {
+    const uint32_t* in;
+    uint64_t in_pitch;  // u32 elements between input rows
+    uint32_t in_rows;   // rows >= in_rows are zero
+    const uint2* pre;   // per input row, or nullptr
+    uint32_t* out;
+    uint64_t out_pitch;  // u32 elements between output rows
+    uint32_t out_rows;   // output rows >= out_rows are not written
+    const uint2* post;   // per output row, or nullptr (then `scale`)
+    Tw scale;
+    uint64_t cols;  // multiple of 4
+};
+
+template <int LOG_N, bool INV>
+__global__ void __launch_bounds__(512, 1)
+    k_coltx(const ColTx a, uint64_t ntiles, const Tw* __restrict__ tw) {
+    using PL = ExtPlan<LOG_N>;
+    extern __shared__ uint4 sm[];
+    const int tid = threadIdx.x;
+    const int q = tid % PL::Q4;
+    const int t = tid / PL::Q4;
+    V4 v[PL::EPT];
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint64_t col = tile * PL::C + 4 * (uint64_t)q;
+        const bool active = col < a.cols;
+        constexpr int R0 = 1 << PL::lr(0);
+        constexpr int L0 = PL::S / R0;
+#pragma unroll
+        for (int j = 0; j < R0; j++) {
+            const uint32_t row = (uint32_t)t + (uint32_t)L0 * j;
+            // a zero pre-factor (an erased row) skips the load
+            const uint2 u = a.pre && row < a.in_rows ? __ldg(a.pre + row) : make_uint2(1u, 0u);
+            if (active && row < a.in_rows && u.x != 0) {
+                v[j] = ldg_stream_v4(a.in + (uint64_t)row * a.in_pitch + col);
+                if (a.pre) mul4(v[j], Tw{u.x, u.y});
+            } else {
+                v[j] = V4{{0, 0, 0, 0}};
+            }
+        }
+        dif_levels<PL, 0, INV>(v, sm, t, q, tw);
+        using LV = Level<PL, PL::lr(PL::NLEV - 1), PL::pre(PL::NLEV - 1)>;
+#pragma unroll
+        for (int g = 0; g < LV::G; g++) {
+            const uint32_t blk = LV::gid(g, t);
+#pragma unroll
+            for (int r = 0; r < LV::R; r++) {
+                const uint32_t k = digit_rev<PL, false>((blk << PL::lr(PL::NLEV - 1)) +
+                                                        (uint32_t)bitrev(r, PL::lr(PL::NLEV - 1)));
+                if (active && k < a.out_rows) {
+                    V4 x = v[g * LV::R + r];
+                    if (a.post) {
+                        const uint2 u = __ldg(a.post + k);
+                        mul4(x, Tw{u.x, u.y});
+                    } else {
+                        mul4(x, a.scale);
+                    }
+                    stg_stream_v4(a.out + (uint64_t)k * a.out_pitch + col, x);
+                }
+            }
+        }
+    }
+}
+
+}  // namespace zb

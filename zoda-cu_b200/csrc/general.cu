@@ -1,0 +1,369 @@
+// Encode of any shape (k data rows, n parity rows) and the k-of-2k erasure
+// decoder, both built on the general column transform (coltx.cuh).
+//
+// Encode, as the reference defines it (src/benchmarks/utils.rs:42-48,100-146,
+// src/zoda/babybear.rs:137-152): n_k = next_pow2(k), n_kn = next_pow2(k + n);
+// the k rows are zero-padded to n_k, interpolated (INTT over n_k), zero-padded
+// to n_kn coefficients and evaluated (NTT over n_kn); the encoding is output
+// rows 0 .. k+n-1 in natural order. With R = n_kn / n_k, output row R*m + c is
+//   c = 0:  the padded data row m (a copy),
+//   c > 0:  NTT_{n_k}(omega_{n_kn}^(c*i) * coef_i)[m], one transform per coset.
+// Square power-of-two inputs (n = k) go to the fused extension kernels instead.
+//
+// Decoder: f of degree < k is known at a set K of the 2k points omega_2k^j.
+// With Z(x) = prod over the erased points of (x - omega^e), g = f * Z has
+// degree < 2k and is known everywhere (zero at the erased points), so
+//   G   = INTT_2k(y_j * Z(omega^j))                    coefficients of g
+//   g~  = NTT_2k(G_i * h^i)                            g on the coset h*omega^j
+//   F~  = INTT_2k(g~_j / Z(h * omega^j))               coefficients of f(h x)
+//   row = NTT_k(F~_i * h^-i), i < k                     f at omega_k^m = data row m
+// with h = 31 (a generator of F_p^*, never a 2k-th root of unity, so Z(h w) != 0).
+// F~_i must vanish for i >= k when the known rows are one codeword; the
+// optional check counts the entries that do not.
+#include <algorithm>
+#include <vector>
+
+#include "coltx.cuh"
+#include "internal.hpp"
+
+namespace zb {
+namespace {
+
+constexpr uint64_t SCRATCH_ELEMS = 64ull << 20;  // u32 per scratch matrix (256 MiB)
+
+int log2_exact64(uint64_t x) {
+    if (x == 0 || (x & (x - 1))) return -1;
+    int l = 0;
+    while ((1ull << l) < x) l++;
+    return l;
+}
+uint64_t next_pow2_64(uint64_t x) {
+    uint64_t r = 1;
+    while (r < x) r <<= 1;
+    return r;
+}
+inline uint2 shoup_pair(uint32_t w) { return make_uint2(w, shoup(w)); }
+
+template <int LOG_N, bool INV>
+zoda_status coltx_t(const zoda_ctx* ctx, const ColTx& a, cudaStream_t st) {
+    using PL = ExtPlan<LOG_N>;
+    const uint64_t ntiles = (a.cols + PL::C - 1) / PL::C;
+    if (ntiles == 0 || a.out_rows == 0) return ZODA_OK;
+    if (PL::SMEM > 0)
+        ZB_CUDA(cudaFuncSetAttribute(k_coltx<LOG_N, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PL::SMEM));
+    const uint64_t grid = ntiles < (uint64_t)ctx->sm_count ? ntiles : (uint64_t)ctx->sm_count;
+    k_coltx<LOG_N, INV><<<(unsigned)grid, PL::THREADS, PL::SMEM, st>>>(a, ntiles, ctx->tables.tw);
+    ZB_CUDA(cudaGetLastError());
+    return ZODA_OK;
+}
+
+// Column transform of size 2^log_n (1 <= log_n <= 12).
+zoda_status coltx(const zoda_ctx* ctx, int log_n, bool inv, const ColTx& a, cudaStream_t st) {
+    switch (log_n) {
+#define ZB_CASE(L) \
+    case L: return inv ? coltx_t<L, true>(ctx, a, st) : coltx_t<L, false>(ctx, a, st);
+        ZB_CASE(1) ZB_CASE(2) ZB_CASE(3) ZB_CASE(4) ZB_CASE(5) ZB_CASE(6)
+        ZB_CASE(7) ZB_CASE(8) ZB_CASE(9) ZB_CASE(10) ZB_CASE(11) ZB_CASE(12)
+#undef ZB_CASE
+        default: return ZODA_ERR_UNSUPPORTED;
+    }
+}
+
+// out[r * pitch + c] = in[c] for r in [0, rows), c in [0, cols).
+__global__ void k_bcast_rows(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint64_t pitch,
+                             uint32_t rows, uint64_t cols) {
+    const uint64_t n = (uint64_t)rows * cols;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t r = i / cols, c = i - r * cols;
+        out[r * pitch + c] = in[c];
+    }
+}
+
+__device__ __forceinline__ uint32_t pow_slow(uint32_t b, uint32_t e) {
+    uint32_t r = 1;
+    while (e) {
+        if (e & 1) r = mul_slow(r, b);
+        b = mul_slow(b, b);
+        e >>= 1;
+    }
+    return r;
+}
+__device__ __forceinline__ uint2 shoup_pair_dev(uint32_t w) {
+    return make_uint2(w, (uint32_t)(((uint64_t)w << 32) / P));
+}
+
+// Decoder tables for one erasure pattern over N = 2^log_n points (see the top
+// of this file); roots[e] = omega_N^e for the erased e:
+//   zk[j]  = Z(omega^j)          (0 at erased j)
+//   hp[i]  = h^i
+//   izh[j] = 1 / Z(h * omega^j)
+//   hm[i]  = h^-i
+__global__ void k_erasure_tables(const uint32_t* __restrict__ erased_roots, uint32_t ne, int log_n,
+                                 const Tw* __restrict__ tw, uint2* __restrict__ zk, uint2* __restrict__ hp,
+                                 uint2* __restrict__ izh, uint2* __restrict__ hm) {
+    const uint32_t N = 1u << log_n;
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= N) return;
+    const uint32_t x = tw[(size_t)j << (LOG_TW - log_n)].w;  // omega_N^j
+    const uint32_t y = mul_slow(GENERATOR, x);
+    uint32_t zx = 1, zy = 1;
+    for (uint32_t i = 0; i < ne; i++) {
+        const uint32_t r = erased_roots[i];
+        zx = mul_slow(zx, x >= r ? x - r : x + P - r);
+        zy = mul_slow(zy, y >= r ? y - r : y + P - r);
+    }
+    zk[j] = shoup_pair_dev(zx);
+    izh[j] = shoup_pair_dev(pow_slow(zy, P - 2));
+    const uint32_t hj = pow_slow(GENERATOR, j);
+    hp[j] = shoup_pair_dev(hj);
+    hm[j] = shoup_pair_dev(pow_slow(hj, P - 2));
+}
+
+// *count += number of nonzero entries of rows [0, rows) x cols (pitch elements apart)
+__global__ void k_count_nonzero(const uint32_t* __restrict__ a, uint64_t pitch, uint32_t rows, uint64_t cols,
+                                unsigned long long* __restrict__ count) {
+    const uint64_t n = (uint64_t)rows * cols;
+    unsigned long long c = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t r = i / cols, cc = i - r * cols;
+        c += a[r * pitch + cc] != 0;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xFFFFFFFFu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+}
+
+unsigned grid_for(const zoda_ctx* ctx, uint64_t n) {
+    const uint64_t g = (n + 255) / 256;
+    const uint64_t cap = (uint64_t)ctx->sm_count * 8;
+    return (unsigned)(g < 1 ? 1 : g > cap ? cap : g);
+}
+
+// Scratch of one chunk: w columns of `rows` rows per matrix.
+uint64_t chunk_cols(uint64_t cols, uint64_t rows) {
+    uint64_t w = SCRATCH_ELEMS / rows;
+    w &= ~3ull;
+    if (w < 4) w = 4;
+    return w < cols ? w : cols;
+}
+
+// Orders this call's use of the context scratch after the previous call's,
+// whichever streams the two calls used.
+zoda_status gen_begin(zoda_ctx* ctx, cudaStream_t st) {
+    if (!ctx->gen_done) {
+        ZB_CUDA(cudaEventCreateWithFlags(&ctx->gen_done, cudaEventDisableTiming));
+        return ZODA_OK;
+    }
+    ZB_CUDA(cudaStreamWaitEvent(st, ctx->gen_done, 0));
+    return ZODA_OK;
+}
+zoda_status gen_end(zoda_ctx* ctx, cudaStream_t st) {
+    ZB_CUDA(cudaEventRecord(ctx->gen_done, st));
+    return ZODA_OK;
+}
+
+// omega_{n_kn}^(c*i) for c in [0, R), i in [0, n_k), row c at c * n_k; built once per shape.
+zoda_status coset_table(zoda_ctx* ctx, int lp, int ln, const uint2** out) {
+    const int key = lp * 64 + ln;
+    DevBuf& b = ctx->coset_tabs[key];
+    const uint64_t P_ = 1ull << lp, R = 1ull << (ln - lp);
+    if (!b.p) {
+        std::vector<uint2> h(R * P_);
+        const uint32_t wn = root_of_unity(ln);
+        for (uint64_t c = 0; c < R; c++) {
+            const uint32_t step = powmod_c(wn, c);
+            uint32_t x = 1;
+            for (uint64_t i = 0; i < P_; i++) {
+                h[c * P_ + i] = shoup_pair(x);
+                x = mulmod_c(x, step);
+            }
+        }
+        zoda_status s = b.ensure(h.size() * sizeof(uint2));
+        if (s != ZODA_OK) return s;
+        ZB_CUDA(cudaMemcpy(b.p, h.data(), h.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+    }
+    *out = (const uint2*)b.p;
+    return ZODA_OK;
+}
+
+zoda_status encode_general(zoda_ctx* ctx, const uint32_t* in, uint32_t* out, uint32_t k, uint32_t n, uint64_t cols,
+                           cudaStream_t st) {
+    const uint64_t P_ = next_pow2_64(k), N = next_pow2_64((uint64_t)k + n), rows_out = (uint64_t)k + n;
+    const int lp = log2_exact64(P_), ln = log2_exact64(N);
+    const uint64_t R = N / P_;
+    const uint64_t rb = cols * 4;  // row bytes
+    // c = 0 rows: R*m for m < ceil(rows_out / R); data rows first, then zero rows
+    const uint64_t m0 = (rows_out + R - 1) / R;
+    const uint64_t mdata = std::min<uint64_t>(k, m0);
+    ZB_CUDA(cudaMemcpy2DAsync(out, R * rb, in, rb, rb, mdata, cudaMemcpyDeviceToDevice, st));
+    if (m0 > mdata) ZB_CUDA(cudaMemset2DAsync(out + R * mdata * cols, R * rb, 0, rb, m0 - mdata, st));
+    if (R == 1) return ZODA_OK;
+    if (P_ == 1) {  // every coset row is the single data row
+        for (uint64_t c = 1; c < R && c < rows_out; c++) {
+            const uint32_t mc = (uint32_t)((rows_out - c + R - 1) / R);
+            k_bcast_rows<<<grid_for(ctx, (uint64_t)mc * cols), 256, 0, st>>>(in, out + c * cols, R * cols, mc, cols);
+            ZB_CUDA(cudaGetLastError());
+        }
+        return ZODA_OK;
+    }
+    const uint2* tabs = nullptr;
+    zoda_status s = coset_table(ctx, lp, ln, &tabs);
+    if (s != ZODA_OK) return s;
+    const uint64_t w0 = chunk_cols(cols, P_);
+    if ((s = ctx->gen_a.ensure(P_ * w0 * 4)) != ZODA_OK) return s;
+    uint32_t* A = (uint32_t*)ctx->gen_a.p;
+    const uint32_t pinv = powmod_c((uint32_t)P_, P - 2);
+    for (uint64_t c0 = 0; c0 < cols; c0 += w0) {
+        const uint64_t w = std::min(w0, cols - c0);
+        // coefficients of the zero-padded data: INTT over n_k, scaled by n_k^-1
+        ColTx a{in + c0, cols, k, nullptr, A, w, (uint32_t)P_, nullptr, Tw{pinv, shoup(pinv)}, w};
+        if ((s = coltx(ctx, lp, true, a, st)) != ZODA_OK) return s;
+        for (uint64_t c = 1; c < R && c < rows_out; c++) {
+            const uint64_t mc = std::min<uint64_t>(P_, (rows_out - c + R - 1) / R);
+            ColTx b{A, w, (uint32_t)P_, tabs + c * P_, out + c * cols + c0, R * cols, (uint32_t)mc, nullptr,
+                    Tw{1u, shoup(1u)}, w};
+            if ((s = coltx(ctx, lp, false, b, st)) != ZODA_OK) return s;
+        }
+    }
+    return ZODA_OK;
+}
+
+}  // namespace
+
+void general_release(zoda_ctx* ctx) {
+    ctx->gen_a.release();
+    ctx->gen_b.release();
+    ctx->gen_tab.release();
+    ctx->gen_small.release();
+    for (auto& kv : ctx->coset_tabs) kv.second.release();
+    ctx->coset_tabs.clear();
+    if (ctx->gen_done) cudaEventDestroy(ctx->gen_done);
+    ctx->gen_done = nullptr;
+}
+
+}  // namespace zb
+
+using namespace zb;
+
+extern "C" {
+
+zoda_status zoda_encode_device(zoda_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t k, uint32_t n,
+                               uint64_t cols, void* stream) {
+    if (!ctx || !d_in || !d_out || k == 0 || cols % 4 != 0) return ZODA_ERR_ARG;
+    if (((uintptr_t)d_in | (uintptr_t)d_out) & 15) return ZODA_ERR_ARG;
+    const uint64_t rows_out = (uint64_t)k + n;
+    const char* a = (const char*)d_in;
+    const char* b = (const char*)d_out;
+    if (cols && a < b + rows_out * cols * 4 && b < a + (uint64_t)k * cols * 4) return ZODA_ERR_ARG;  // overlap
+    if (next_pow2_64(k) > zoda_max_side() || rows_out > (1ull << 27)) {
+        set_last_error_text("encode supports next_pow2(k) <= 4096 and k + n <= 2^27");
+        return ZODA_ERR_UNSUPPORTED;
+    }
+    if (n == k && log2_exact64(k) >= 0) return zoda_extend_device(ctx, d_in, d_out, k, cols, stream);
+    if (cols == 0) return ZODA_OK;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ZB_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    zoda_status s = gen_begin(ctx, st);
+    if (s != ZODA_OK) return s;
+    s = encode_general(ctx, d_in, d_out, k, n, cols, st);
+    zoda_status e = gen_end(ctx, st);
+    return s != ZODA_OK ? s : e;
+}
+
+zoda_status zoda_recover_device(zoda_ctx* ctx, const uint32_t* d_code, const uint32_t* known_rows, uint32_t nknown,
+                                uint32_t k, uint64_t cols, uint32_t* d_data, uint64_t* mismatch, void* stream) {
+    if (!ctx || !d_code || !d_data || !known_rows || cols % 4 != 0) return ZODA_ERR_ARG;
+    if (((uintptr_t)d_code | (uintptr_t)d_data) & 15) return ZODA_ERR_ARG;
+    const int lk = log2_exact64(k);
+    if (lk < 0) return ZODA_ERR_ARG;
+    if (lk > 11) {
+        set_last_error_text("the decoder covers k <= 2048 (codewords of up to 4096 rows)");
+        return ZODA_ERR_UNSUPPORTED;
+    }
+    const uint32_t N = 2 * k;
+    const int ln = lk + 1;
+    std::vector<uint8_t> have(N, 0);
+    for (uint32_t i = 0; i < nknown; i++) {
+        if (known_rows[i] >= N) return ZODA_ERR_ARG;
+        have[known_rows[i]] = 1;
+    }
+    uint32_t nk = 0;
+    for (uint8_t h : have) nk += h;
+    if (nk < k) {
+        set_last_error_text("fewer than k distinct known rows");
+        return ZODA_ERR_ARG;
+    }
+    const char* a = (const char*)d_code;
+    const char* b = (const char*)d_data;
+    if (cols && a < b + (uint64_t)k * cols * 4 && b < a + (uint64_t)N * cols * 4) return ZODA_ERR_ARG;  // overlap
+    if (mismatch) *mismatch = 0;
+    if (cols == 0) return ZODA_OK;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ZB_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    zoda_status s = gen_begin(ctx, st);
+    if (s != ZODA_OK) return s;
+    auto finish = [&](zoda_status r) {
+        zoda_status e = gen_end(ctx, st);
+        return r != ZODA_OK ? r : e;
+    };
+    bool evens = true;
+    for (uint32_t m = 0; m < k; m++) evens = evens && have[2 * m];
+    const uint64_t rb = cols * 4;
+    if (evens && !mismatch) {  // the data rows are all there
+        ZB_CUDA(cudaMemcpy2DAsync(d_data, rb, d_code, 2 * rb, rb, k, cudaMemcpyDeviceToDevice, st));
+        return finish(ZODA_OK);
+    }
+    // pattern tables: roots of the erased points, then zk | hp | izh | hm
+    std::vector<uint32_t> er;
+    const uint32_t wn = root_of_unity(ln);
+    for (uint32_t j = 0, x = 1; j < N; j++, x = mulmod_c(x, wn))
+        if (!have[j]) er.push_back(x);
+    if ((s = ctx->gen_tab.ensure((size_t)4 * N * sizeof(uint2))) != ZODA_OK) return finish(s);
+    if ((s = ctx->gen_small.ensure(std::max<size_t>(1, er.size()) * 4 + 64)) != ZODA_OK) return finish(s);
+    uint2* T = (uint2*)ctx->gen_tab.p;
+    uint2 *zk = T, *hp = T + N, *izh = T + 2 * N, *hm = T + 3 * N;
+    uint32_t* d_er = (uint32_t*)ctx->gen_small.p;
+    unsigned long long* d_cnt = (unsigned long long*)((char*)ctx->gen_small.p + ((er.size() * 4 + 15) / 16) * 16);
+    if (!er.empty())
+        ZB_CUDA(cudaMemcpyAsync(d_er, er.data(), er.size() * 4, cudaMemcpyHostToDevice, st));
+    k_erasure_tables<<<(N + 127) / 128, 128, 0, st>>>(d_er, (uint32_t)er.size(), ln, ctx->tables.tw, zk, hp, izh, hm);
+    ZB_CUDA(cudaGetLastError());
+    if (mismatch) ZB_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), st));
+    const uint64_t w0 = chunk_cols(cols, N);
+    if ((s = ctx->gen_a.ensure((uint64_t)N * w0 * 4)) != ZODA_OK) return finish(s);
+    if ((s = ctx->gen_b.ensure((uint64_t)N * w0 * 4)) != ZODA_OK) return finish(s);
+    uint32_t* A = (uint32_t*)ctx->gen_a.p;
+    uint32_t* B = (uint32_t*)ctx->gen_b.p;
+    const uint32_t ninv = powmod_c(N, P - 2);
+    const Tw sc_inv{ninv, shoup(ninv)}, one{1u, shoup(1u)};
+    for (uint64_t c0 = 0; c0 < cols; c0 += w0) {
+        const uint64_t w = std::min(w0, cols - c0);
+        const ColTx p1{d_code + c0, cols, N, zk, A, w, N, nullptr, sc_inv, w};
+        const ColTx p2{A, w, N, hp, B, w, N, nullptr, one, w};
+        const ColTx p3{B, w, N, izh, A, w, mismatch ? N : k, nullptr, sc_inv, w};
+        if ((s = coltx(ctx, ln, true, p1, st)) != ZODA_OK) return finish(s);
+        if ((s = coltx(ctx, ln, false, p2, st)) != ZODA_OK) return finish(s);
+        if ((s = coltx(ctx, ln, true, p3, st)) != ZODA_OK) return finish(s);
+        if (lk == 0) {
+            ZB_CUDA(cudaMemcpy2DAsync(d_data + c0, rb, A, w * 4, w * 4, 1, cudaMemcpyDeviceToDevice, st));
+        } else {
+            const ColTx p4{A, w, k, hm, d_data + c0, cols, k, nullptr, one, w};
+            if ((s = coltx(ctx, lk, false, p4, st)) != ZODA_OK) return finish(s);
+        }
+        if (mismatch) {
+            k_count_nonzero<<<grid_for(ctx, (uint64_t)k * w), 256, 0, st>>>(A + (uint64_t)k * w, w, k, w, d_cnt);
+            ZB_CUDA(cudaGetLastError());
+        }
+    }
+    if (mismatch) {
+        unsigned long long h = 0;
+        ZB_CUDA(cudaMemcpyAsync(&h, d_cnt, sizeof h, cudaMemcpyDeviceToHost, st));
+        ZB_CUDA(cudaStreamSynchronize(st));
+        *mismatch = h;
+    }
+    return finish(ZODA_OK);
+}
+
+}  // extern "C"

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
 #include <mutex>
 #include <string>
 
@@ -61,6 +62,12 @@ struct zoda_ctx {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t cev[MAX_CHUNKS][4] = {};
     std::mutex mu;  // serialises host calls on one context
+    // encode of any (k, n) and erasure decoder (general.cu): two column-chunk
+    // scratch matrices, per-pattern tables, coset twist tables keyed by
+    // (log2 n_k, log2 n_kn), and an event after each call's last use of them
+    zb::DevBuf gen_a, gen_b, gen_tab, gen_small;
+    std::map<int, zb::DevBuf> coset_tabs;
+    cudaEvent_t gen_done = nullptr;
 };
 
 namespace zb {
@@ -70,4 +77,6 @@ zoda_status launch_extend(const zoda_ctx* ctx, int log_s, const uint32_t* in, ui
                           cudaStream_t st, int impl = 0);
 // Sets the dynamic shared memory attribute of every extension instantiation.
 zoda_status extend_init_attributes();
+// Frees what the general encode / decoder left in the context.
+void general_release(zoda_ctx* ctx);
 }  // namespace zb

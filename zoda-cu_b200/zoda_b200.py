@@ -35,6 +35,7 @@ EXPORTS = [
     "zoda_ntt_device_noalloc", "zoda_batch_create", "zoda_batch_run", "zoda_batch_elements",
     "zoda_batch_destroy", "zoda_server_create", "zoda_server_submit", "zoda_server_wait",
     "zoda_server_release", "zoda_server_cancel", "zoda_server_get_stats", "zoda_server_destroy",
+    "zoda_encode_device", "zoda_recover_device",
 ]
 
 _lib = None
@@ -129,6 +130,11 @@ def load(path: str = LIB_PATH):
     L.zoda_server_get_stats.argtypes = [vp, ctypes.POINTER(ZodaServerStats)]
     L.zoda_server_destroy.restype = None
     L.zoda_server_destroy.argtypes = [vp]
+    L.zoda_encode_device.restype = ctypes.c_int
+    L.zoda_encode_device.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, vp]
+    L.zoda_recover_device.restype = ctypes.c_int
+    L.zoda_recover_device.argtypes = [vp, vp, u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, vp,
+                                      ctypes.POINTER(ctypes.c_uint64), vp]
     L.zoda_ntt_device_noalloc.restype = ctypes.c_int
     L.zoda_ntt_device_noalloc.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, vp]
     L.zoda_extend_host.restype = ctypes.c_int
@@ -190,6 +196,24 @@ class Context:
         s = stream if isinstance(stream, int) else stream.cuda_stream
         _check(load().zoda_extend_device(self._h, _addr(d_in), _addr(d_out), k, cols, s or None),
                "zoda_extend_device")
+
+    def encode(self, d_in, d_out, k: int, n: int, cols: int, stream=None):
+        """Encode of any shape (src/benchmarks/utils.rs:100-146): d_in [k][cols] ->
+        d_out [k+n][cols], rows 0..k+n-1 of the evaluation over next_pow2(k+n) points."""
+        _check(load().zoda_encode_device(self._h, _addr(d_in), _addr(d_out), k, n, cols, _stream_handle(stream)),
+               "zoda_encode_device")
+
+    def recover(self, d_code, known_rows, k: int, cols: int, d_data, check: bool = False, stream=None):
+        """k-of-2k erasure recovery: d_code [2k][cols] with only `known_rows` valid ->
+        d_data [k][cols]. With check=True returns the number of inconsistent
+        coefficients (0 when the known rows are one codeword) and synchronizes."""
+        rows = sorted(set(int(r) for r in known_rows))
+        arr = (ctypes.c_uint32 * max(1, len(rows)))(*rows)
+        mm = ctypes.c_uint64(0)
+        _check(load().zoda_recover_device(self._h, _addr(d_code), arr, len(rows), k, cols, _addr(d_data),
+                                          ctypes.byref(mm) if check else None, _stream_handle(stream)),
+               "zoda_recover_device")
+        return int(mm.value) if check else None
 
     def set_impl(self, impl: int):
         """0 = automatic, 1 = direct-load kernel, 2 = TMA-staged kernel."""
