@@ -98,6 +98,38 @@ typedef enum zoda_extend_impl {
 } zoda_extend_impl;
 zoda_status zoda_ctx_set_impl(zoda_ctx* ctx, int impl);
 
+/* Per-side launch plan of the fused extension. No counterpart in the
+ * reference, whose kernel shape is fixed (cuda/ntt_kernel.cu:130-160). With
+ * ZODA_IMPL_AUTO a side that has a plan (from zoda_autotune or
+ * zoda_plan_set) runs that plan; a side without one runs the default plan
+ * (TMA for 128 <= k <= 2048, else direct; sched 0, l2_promo 3, blocked 0,
+ * stagger 1). Every plan computes the same bits; only the speed differs. */
+typedef struct zoda_plan {
+    int32_t impl;     /* ZODA_IMPL_DIRECT or ZODA_IMPL_TMA (k >= 32)                   */
+    int32_t sched;    /* direct kernel: radix-16 levels with the leftover radix at the
+                         INTT's last level (0) or its first level (1)                  */
+    int32_t l2_promo; /* TMA kernel: L2 promotion of tile loads, 0 none, 1 64 B,
+                         2 128 B, 3 256 B                                              */
+    int32_t blocked;  /* 0 = CTA i takes tiles i, i + grid, ...; 1 = one contiguous run */
+    int32_t stagger;  /* TMA kernel: 1 = the two warp-groups run half a tile apart     */
+    float ms;         /* the tuner's time for this plan (0 when set by hand)            */
+} zoda_plan;
+
+/* Times every candidate plan for each power-of-two side in [side_min,
+ * side_max] (sides 1..4096) on a synthetic [side][cols] square
+ * (cols = 0: about 256 MiB of input, rounded to the side's tile width), with
+ * `reps` timed runs after one warm-up. A candidate whose output differs in
+ * any bit from the default plan's is rejected. The fastest is installed on
+ * the context and written to plans[log2(side)] when `plans` is not NULL
+ * (an array of 13). Allocates and frees its own buffers; synchronous. */
+zoda_status zoda_autotune(zoda_ctx* ctx, uint32_t side_min, uint32_t side_max, uint64_t cols, uint32_t reps,
+                          zoda_plan* plans);
+/* Reads (ZODA_ERR_STATE when the side has no plan) or installs the plan of
+ * one side, e.g. from a saved tuning file; zoda_plan_clear drops them all. */
+zoda_status zoda_plan_get(const zoda_ctx* ctx, uint32_t side, zoda_plan* plan);
+zoda_status zoda_plan_set(zoda_ctx* ctx, uint32_t side, const zoda_plan* plan);
+void zoda_plan_clear(zoda_ctx* ctx);
+
 /* Returns ZODA_ERR_TIMEOUT (and clears the flag) if a kernel on this context
  * gave up a bounded wait since the last call, else ZODA_OK. Synchronizes the
  * device first. */

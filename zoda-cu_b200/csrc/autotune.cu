@@ -1,0 +1,220 @@
+// Per-side autotuner of the fused extension (zoda_autotune, zoda_plan_*).
+//
+// For each side the tuner builds a synthetic square, runs the default plan
+// once as the bit-for-bit reference, then for every candidate plan:
+// fills the output with 0xFFFFFFFF (never a canonical value), runs the
+// candidate once, counts the words that differ from the reference on the
+// device (a candidate with any difference is rejected), and times `reps`
+// back-to-back launches with CUDA events on the context's stream. The
+// fastest survivor becomes the side's plan on the context.
+//
+// Candidates: the direct-load kernel with either radix schedule and either
+// tile order; the TMA-staged kernel (sides >= 32) with L2 promotion 256 B,
+// 128 B or none, either tile order, with and without the warp-group stagger.
+#include <algorithm>
+#include <vector>
+
+#include "internal.hpp"
+
+namespace zb {
+namespace {
+
+// seeded values in [0, p) (splitmix64 of the index)
+__global__ void k_fill(uint32_t* __restrict__ a, uint64_t n, uint64_t seed) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t z = (i + seed) * 0x9E3779B97F4A7C15ull;
+        z ^= z >> 30;
+        z *= 0xBF58476D1CE4E5B9ull;
+        z ^= z >> 27;
+        z *= 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        a[i] = (uint32_t)(z % P);
+    }
+}
+
+// *diff += number of positions where a and b differ
+__global__ void k_diff(const uint4* __restrict__ a, const uint4* __restrict__ b, uint64_t n4,
+                       unsigned long long* __restrict__ diff) {
+    unsigned long long c = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n4; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint4 x = a[i], y = b[i];
+        c += (x.x != y.x) + (x.y != y.y) + (x.z != y.z) + (x.w != y.w);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xFFFFFFFFu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(diff, c);
+}
+
+constexpr bool distinct_sched1(int ls) { return ls >= 5 && ls % 4 != 0; }
+
+std::vector<zoda_plan> candidates(int ls) {
+    std::vector<zoda_plan> c;
+    const zoda_plan d = default_plan(ls);
+    c.push_back(d);
+    auto same = [](const zoda_plan& a, const zoda_plan& b) {
+        return a.impl == b.impl && a.sched == b.sched && a.l2_promo == b.l2_promo && a.blocked == b.blocked &&
+               a.stagger == b.stagger;
+    };
+    auto add = [&](zoda_plan p) {
+        for (const auto& q : c)
+            if (same(p, q)) return;
+        c.push_back(p);
+    };
+    for (int blocked = 0; blocked <= 1; blocked++) {
+        for (int sched = 0; sched <= (distinct_sched1(ls) ? 1 : 0); sched++) {
+            zoda_plan p = d;
+            p.impl = ZODA_IMPL_DIRECT;
+            p.sched = sched;
+            p.blocked = blocked;
+            p.l2_promo = 3;
+            p.stagger = 1;
+            add(p);
+        }
+        if (ls >= 5)
+            for (int promo : {3, 2, 0})
+                for (int stagger = 1; stagger >= 0; stagger--) {
+                    zoda_plan p = d;
+                    p.impl = ZODA_IMPL_TMA;
+                    p.sched = 0;
+                    p.l2_promo = promo;
+                    p.blocked = blocked;
+                    p.stagger = stagger;
+                    add(p);
+                }
+    }
+    return c;
+}
+
+struct TuneBufs {
+    void *in = nullptr, *ref = nullptr, *out = nullptr, *cnt = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    ~TuneBufs() {
+        if (in) cudaFree(in);
+        if (ref) cudaFree(ref);
+        if (out) cudaFree(out);
+        if (cnt) cudaFree(cnt);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    }
+};
+
+unsigned small_grid(const zoda_ctx* ctx, uint64_t n) {
+    const uint64_t g = (n + 255) / 256, cap = (uint64_t)ctx->sm_count * 8;
+    return (unsigned)(g < 1 ? 1 : g > cap ? cap : g);
+}
+
+zoda_status tune_side(zoda_ctx* ctx, int ls, uint64_t cols, uint32_t reps, zoda_plan* best_out) {
+    const uint64_t S = 1ull << ls;
+    if (cols == 0) {
+        cols = (64ull << 20) / S;
+        cols -= cols % 2048;
+        if (cols < 2048) cols = 2048;
+    }
+    cudaStream_t st = ctx->stream;
+    TuneBufs b;
+    const uint64_t nin = S * cols, nout = 2 * S * cols;
+    ZB_CUDA(cudaMalloc(&b.in, nin * 4));
+    ZB_CUDA(cudaMalloc(&b.ref, nout * 4));
+    ZB_CUDA(cudaMalloc(&b.out, nout * 4));
+    ZB_CUDA(cudaMalloc(&b.cnt, sizeof(unsigned long long)));
+    ZB_CUDA(cudaEventCreate(&b.e0));
+    ZB_CUDA(cudaEventCreate(&b.e1));
+    k_fill<<<small_grid(ctx, nin), 256, 0, st>>>((uint32_t*)b.in, nin, 0x5eed0000ull + (uint64_t)ls);
+    ZB_CUDA(cudaGetLastError());
+    const uint32_t* in = (const uint32_t*)b.in;
+    const std::vector<zoda_plan> cand = candidates(ls);
+    zoda_status s = launch_plan(ctx, ls, cand[0], in, (uint32_t*)b.ref, cols, st);
+    if (s != ZODA_OK) return s;
+    zoda_plan best{};
+    float best_ms = 0.f;
+    bool have = false;
+    for (const zoda_plan& p : cand) {
+        ZB_CUDA(cudaMemsetAsync(b.out, 0xFF, nout * 4, st));
+        if ((s = launch_plan(ctx, ls, p, in, (uint32_t*)b.out, cols, st)) != ZODA_OK) return s;
+        ZB_CUDA(cudaMemsetAsync(b.cnt, 0, sizeof(unsigned long long), st));
+        k_diff<<<small_grid(ctx, nout / 4), 256, 0, st>>>((const uint4*)b.out, (const uint4*)b.ref, nout / 4,
+                                                          (unsigned long long*)b.cnt);
+        ZB_CUDA(cudaGetLastError());
+        unsigned long long diff = 0;
+        ZB_CUDA(cudaMemcpyAsync(&diff, b.cnt, sizeof diff, cudaMemcpyDeviceToHost, st));
+        ZB_CUDA(cudaStreamSynchronize(st));
+        if (diff != 0) continue;  // not bit-exact with the default plan: never chosen
+        ZB_CUDA(cudaEventRecord(b.e0, st));
+        for (uint32_t r = 0; r < reps; r++)
+            if ((s = launch_plan(ctx, ls, p, in, (uint32_t*)b.out, cols, st)) != ZODA_OK) return s;
+        ZB_CUDA(cudaEventRecord(b.e1, st));
+        ZB_CUDA(cudaEventSynchronize(b.e1));
+        float ms = 0.f;
+        ZB_CUDA(cudaEventElapsedTime(&ms, b.e0, b.e1));
+        ms /= (float)reps;
+        if (!have || ms < best_ms) {
+            best = p;
+            best_ms = ms;
+            have = true;
+        }
+    }
+    if (!have) {
+        set_last_error_text("autotune: no candidate reproduced the default plan's output");
+        return ZODA_ERR_STATE;
+    }
+    best.ms = best_ms;
+    *best_out = best;
+    return ZODA_OK;
+}
+
+int log2_pow2(uint32_t x) {
+    if (x == 0 || (x & (x - 1))) return -1;
+    int l = 0;
+    while ((1u << l) < x) l++;
+    return l;
+}
+
+}  // namespace
+}  // namespace zb
+
+using namespace zb;
+
+extern "C" {
+
+zoda_status zoda_autotune(zoda_ctx* ctx, uint32_t side_min, uint32_t side_max, uint64_t cols, uint32_t reps,
+                          zoda_plan* plans) {
+    const int lo = log2_pow2(side_min), hi = log2_pow2(side_max);
+    if (!ctx || lo < 0 || hi < 0 || lo > hi || reps == 0 || cols % 4 != 0) return ZODA_ERR_ARG;
+    if (hi > 12) return ZODA_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ZB_CUDA(cudaSetDevice(ctx->device));
+    for (int ls = lo; ls <= hi; ls++) {
+        zoda_plan best{};
+        const zoda_status s = tune_side(ctx, ls, cols, reps, &best);
+        if (s != ZODA_OK) return s;
+        ctx->plan[ls] = best;
+        ctx->planned[ls] = true;
+        if (plans) plans[ls] = best;
+    }
+    return ZODA_OK;
+}
+
+zoda_status zoda_plan_get(const zoda_ctx* ctx, uint32_t side, zoda_plan* plan) {
+    const int ls = log2_pow2(side);
+    if (!ctx || !plan || ls < 0 || ls > 12) return ZODA_ERR_ARG;
+    if (!ctx->planned[ls]) return ZODA_ERR_STATE;
+    *plan = ctx->plan[ls];
+    return ZODA_OK;
+}
+
+zoda_status zoda_plan_set(zoda_ctx* ctx, uint32_t side, const zoda_plan* plan) {
+    const int ls = log2_pow2(side);
+    if (!ctx || !plan || ls < 0 || ls > 12) return ZODA_ERR_ARG;
+    const zoda_status s = check_plan(ls, *plan);
+    if (s != ZODA_OK) return s;
+    ctx->plan[ls] = *plan;
+    ctx->planned[ls] = true;
+    return ZODA_OK;
+}
+
+void zoda_plan_clear(zoda_ctx* ctx) {
+    if (!ctx) return;
+    for (bool& p : ctx->planned) p = false;
+}
+
+}  // extern "C"

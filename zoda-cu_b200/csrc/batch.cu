@@ -28,9 +28,9 @@ namespace zb {
 namespace {
 
 template <int LOG_S>
-zoda_status fill_square(BatchSquare* b, const zoda_square& q) {
+zoda_status fill_square(BatchSquare* b, const zoda_square& q, int promo) {
     using TP = TPlan<LOG_S>;
-    zoda_status s = make_tile_maps<TP>(&b->in_map, &b->even_map, q.d_in, q.d_out, q.cols);
+    zoda_status s = make_tile_maps<TP>(&b->in_map, &b->even_map, q.d_in, q.d_out, q.cols, promo);
     if (s != ZODA_OK) return s;
     b->out = q.d_out;
     b->cols = q.cols;
@@ -48,7 +48,7 @@ int log2_side(uint32_t k) {
 
 }  // namespace
 
-zoda_status make_batch_square(const zoda_square& q, BatchSquare* b) {
+zoda_status make_batch_square(const zoda_square& q, BatchSquare* b, int promo) {
     const int ls = log2_side(q.k);
     if (!q.d_in || !q.d_out || ls < 0 || q.cols % 4 || (((uintptr_t)q.d_in | (uintptr_t)q.d_out) & 15))
         return ZODA_ERR_ARG;
@@ -58,13 +58,13 @@ zoda_status make_batch_square(const zoda_square& q, BatchSquare* b) {
     }
     memset(b, 0, sizeof *b);
     switch (ls) {
-        case 5: return fill_square<5>(b, q);
-        case 6: return fill_square<6>(b, q);
-        case 7: return fill_square<7>(b, q);
-        case 8: return fill_square<8>(b, q);
-        case 9: return fill_square<9>(b, q);
-        case 10: return fill_square<10>(b, q);
-        default: return fill_square<11>(b, q);
+        case 5: return fill_square<5>(b, q, promo);
+        case 6: return fill_square<6>(b, q, promo);
+        case 7: return fill_square<7>(b, q, promo);
+        case 8: return fill_square<8>(b, q, promo);
+        case 9: return fill_square<9>(b, q, promo);
+        case 10: return fill_square<10>(b, q, promo);
+        default: return fill_square<11>(b, q, promo);
     }
 }
 
@@ -100,7 +100,7 @@ zoda_status zoda_batch_create(zoda_ctx* ctx, const zoda_square* squares, uint32_
     for (uint32_t j = 0; j < n; j++) {
         const zoda_square& q = squares[order[j]];
         BatchSquare& b = host[j];
-        const zoda_status s = make_batch_square(q, &b);
+        const zoda_status s = make_batch_square(q, &b, side_l2_promo(ctx, log2_side(q.k)));
         if (s != ZODA_OK) return s;
         b.first = first;
         first += b.ntiles;

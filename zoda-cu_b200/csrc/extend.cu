@@ -16,42 +16,61 @@ __global__ void k_extend_side1(const uint32_t* __restrict__ in, uint32_t* __rest
     }
 }
 
-template <int LOG_S>
-zoda_status launch_t(const zoda_ctx* ctx, const uint32_t* in, uint32_t* out, uint64_t cols, cudaStream_t st) {
-    using PL = ExtPlan<LOG_S>;
+template <int LOG_S, int SCHED>
+zoda_status launch_t(const zoda_ctx* ctx, const uint32_t* in, uint32_t* out, uint64_t cols, uint32_t flags,
+                     cudaStream_t st) {
+    using PL = ExtPlan<LOG_S, SCHED>;
     const uint64_t ntiles = (cols + PL::C - 1) / PL::C;
     if (ntiles == 0) return ZODA_OK;
     const uint64_t grid = ntiles < (uint64_t)ctx->sm_count ? ntiles : (uint64_t)ctx->sm_count;
-    k_extend<LOG_S><<<(unsigned)grid, PL::THREADS, PL::SMEM, st>>>(in, out, cols, ntiles, ctx->tables.tw,
-                                                                   ctx->tables.twist);
+    k_extend<LOG_S, SCHED><<<(unsigned)grid, PL::THREADS, PL::SMEM, st>>>(in, out, cols, ntiles, ctx->tables.tw,
+                                                                          ctx->tables.twist, flags);
     ZB_CUDA(cudaGetLastError());
     return ZODA_OK;
 }
 
 template <int LOG_S>
-zoda_status launch_tma_t(const zoda_ctx* ctx, const uint32_t* in, uint32_t* out, uint64_t cols, cudaStream_t st) {
+zoda_status launch_tma_t(const zoda_ctx* ctx, const uint32_t* in, uint32_t* out, uint64_t cols, int promo,
+                         uint32_t flags, cudaStream_t st) {
     using TP = TPlan<LOG_S>;
     const uint64_t ntiles = (cols + TP::C - 1) / TP::C;
     if (ntiles == 0) return ZODA_OK;
     CUtensorMap m_in, m_even;
-    zoda_status s = make_tile_maps<TP>(&m_in, &m_even, in, out, cols);
+    zoda_status s = make_tile_maps<TP>(&m_in, &m_even, in, out, cols, promo);
     if (s != ZODA_OK) return s;
     const uint64_t grid = ntiles < (uint64_t)ctx->sm_count ? ntiles : (uint64_t)ctx->sm_count;
     const SideTables tb = side_tables(ctx, LOG_S);
-    k_extend_tma<LOG_S><<<(unsigned)grid, 512, TP::SMEM, st>>>(m_in, m_even, out, cols, ntiles, tb, ctx->d_err);
+    k_extend_tma<LOG_S><<<(unsigned)grid, 512, TP::SMEM, st>>>(m_in, m_even, out, cols, ntiles, tb, ctx->d_err,
+                                                               flags);
     ZB_CUDA(cudaGetLastError());
     return ZODA_OK;
 }
 
+// The leftover radix differs from 16 (so schedule 1 is a distinct kernel) for
+// these sides only.
+constexpr bool has_sched1(int ls) { return ls >= 5 && ls % 4 != 0; }
+
 template <int LOG_S>
 zoda_status set_attr_t() {
     using PL = ExtPlan<LOG_S>;
-    if (PL::SMEM > 0)
-        ZB_CUDA(cudaFuncSetAttribute(k_extend<LOG_S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PL::SMEM));
+    if (PL::SMEM > 0) {
+        ZB_CUDA(cudaFuncSetAttribute(k_extend<LOG_S, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PL::SMEM));
+        if constexpr (has_sched1(LOG_S))
+            ZB_CUDA(cudaFuncSetAttribute(k_extend<LOG_S, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)ExtPlan<LOG_S, 1>::SMEM));
+    }
     if constexpr (LOG_S >= 5)
         ZB_CUDA(cudaFuncSetAttribute(k_extend_tma<LOG_S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)TPlan<LOG_S>::SMEM));
     return ZODA_OK;
+}
+
+template <int LOG_S>
+zoda_status launch_direct(const zoda_ctx* ctx, int sched, const uint32_t* in, uint32_t* out, uint64_t cols,
+                          uint32_t flags, cudaStream_t st) {
+    if constexpr (has_sched1(LOG_S))
+        if (sched == 1) return launch_t<LOG_S, 1>(ctx, in, out, cols, flags, st);
+    return launch_t<LOG_S, 0>(ctx, in, out, cols, flags, st);
 }
 }  // namespace
 
@@ -65,23 +84,47 @@ zoda_status extend_init_attributes() {
     return s;
 }
 
-zoda_status launch_extend(const zoda_ctx* ctx, int log_s, const uint32_t* in, uint32_t* out, uint64_t cols,
-                          cudaStream_t st, int impl) {
-    // AUTO: the TMA-staged kernel from side 128 up to 2048; at side 4096 its
+zoda_plan default_plan(int log_s) {
+    // the TMA-staged kernel from side 128 up to 2048; at side 4096 its
     // 8-column tiles split 32-byte sectors between the two warp-groups, and the
-    // direct-load kernel is faster.
-    const bool tma = (impl == 2) || (impl == 0 && log_s >= 7 && log_s <= 11);
-    if (impl == 2 && (log_s < 5 || log_s > 12)) return ZODA_ERR_UNSUPPORTED;
-    if (tma) {
+    // direct-load kernel is faster
+    zoda_plan p{};
+    p.impl = (log_s >= 7 && log_s <= 11) ? ZODA_IMPL_TMA : ZODA_IMPL_DIRECT;
+    p.sched = 0;
+    p.l2_promo = 3;
+    p.blocked = 0;
+    p.stagger = 1;
+    p.ms = 0.f;
+    return p;
+}
+
+zoda_status check_plan(int log_s, const zoda_plan& p) {
+    if (log_s < 0 || log_s > 12) return ZODA_ERR_UNSUPPORTED;
+    if (p.impl != ZODA_IMPL_DIRECT && p.impl != ZODA_IMPL_TMA) return ZODA_ERR_ARG;
+    if (p.impl == ZODA_IMPL_TMA && log_s < 5) return ZODA_ERR_UNSUPPORTED;
+    if (p.sched < 0 || p.sched > 1 || p.l2_promo < 0 || p.l2_promo > 3 || p.blocked < 0 || p.blocked > 1 ||
+        p.stagger < 0 || p.stagger > 1)
+        return ZODA_ERR_ARG;
+    return ZODA_OK;
+}
+
+int side_l2_promo(const zoda_ctx* ctx, int log_s) {
+    if (log_s >= 0 && log_s <= 12 && ctx->planned[log_s] && ctx->plan[log_s].impl == ZODA_IMPL_TMA)
+        return ctx->plan[log_s].l2_promo;
+    return 3;
+}
+
+zoda_status launch_plan(const zoda_ctx* ctx, int log_s, const zoda_plan& p, const uint32_t* in, uint32_t* out,
+                        uint64_t cols, cudaStream_t st) {
+    zoda_status s = check_plan(log_s, p);
+    if (s != ZODA_OK) return s;
+    const uint32_t flags = (p.blocked ? 1u : 0u) | (p.stagger ? 0u : 2u);
+    if (p.impl == ZODA_IMPL_TMA) {
         switch (log_s) {
-            case 5: return launch_tma_t<5>(ctx, in, out, cols, st);
-            case 6: return launch_tma_t<6>(ctx, in, out, cols, st);
-            case 7: return launch_tma_t<7>(ctx, in, out, cols, st);
-            case 8: return launch_tma_t<8>(ctx, in, out, cols, st);
-            case 9: return launch_tma_t<9>(ctx, in, out, cols, st);
-            case 10: return launch_tma_t<10>(ctx, in, out, cols, st);
-            case 11: return launch_tma_t<11>(ctx, in, out, cols, st);
-            case 12: return launch_tma_t<12>(ctx, in, out, cols, st);
+#define ZB_CASE(L) \
+    case L: return launch_tma_t<L>(ctx, in, out, cols, p.l2_promo, flags, st);
+            ZB_CASE(5) ZB_CASE(6) ZB_CASE(7) ZB_CASE(8) ZB_CASE(9) ZB_CASE(10) ZB_CASE(11) ZB_CASE(12)
+#undef ZB_CASE
             default: return ZODA_ERR_UNSUPPORTED;
         }
     }
@@ -93,20 +136,23 @@ zoda_status launch_extend(const zoda_ctx* ctx, int log_s, const uint32_t* in, ui
             ZB_CUDA(cudaGetLastError());
             return ZODA_OK;
         }
-        case 1: return launch_t<1>(ctx, in, out, cols, st);
-        case 2: return launch_t<2>(ctx, in, out, cols, st);
-        case 3: return launch_t<3>(ctx, in, out, cols, st);
-        case 4: return launch_t<4>(ctx, in, out, cols, st);
-        case 5: return launch_t<5>(ctx, in, out, cols, st);
-        case 6: return launch_t<6>(ctx, in, out, cols, st);
-        case 7: return launch_t<7>(ctx, in, out, cols, st);
-        case 8: return launch_t<8>(ctx, in, out, cols, st);
-        case 9: return launch_t<9>(ctx, in, out, cols, st);
-        case 10: return launch_t<10>(ctx, in, out, cols, st);
-        case 11: return launch_t<11>(ctx, in, out, cols, st);
-        case 12: return launch_t<12>(ctx, in, out, cols, st);
+#define ZB_CASE(L) \
+    case L: return launch_direct<L>(ctx, p.sched, in, out, cols, flags, st);
+        ZB_CASE(1) ZB_CASE(2) ZB_CASE(3) ZB_CASE(4) ZB_CASE(5) ZB_CASE(6)
+        ZB_CASE(7) ZB_CASE(8) ZB_CASE(9) ZB_CASE(10) ZB_CASE(11) ZB_CASE(12)
+#undef ZB_CASE
         default: return ZODA_ERR_UNSUPPORTED;
     }
+}
+
+zoda_status launch_extend(const zoda_ctx* ctx, int log_s, const uint32_t* in, uint32_t* out, uint64_t cols,
+                          cudaStream_t st, int impl) {
+    if (log_s < 0 || log_s > 12) return ZODA_ERR_UNSUPPORTED;
+    zoda_plan p = default_plan(log_s);
+    if (impl == ZODA_IMPL_AUTO && ctx->planned[log_s]) p = ctx->plan[log_s];
+    else if (impl == ZODA_IMPL_DIRECT) p.impl = ZODA_IMPL_DIRECT;
+    else if (impl == ZODA_IMPL_TMA) p.impl = ZODA_IMPL_TMA;
+    return launch_plan(ctx, log_s, p, in, out, cols, st);
 }
 
 }  // namespace zb

@@ -26,9 +26,13 @@ namespace zb {
 constexpr int LOG_TW = 13;  // global twiddle table: omega_8192^j, covers 2S up to 8192
 constexpr int TW_N = 1 << LOG_TW;
 
-template <int LOG_S_>
+// SCHED picks where the leftover radix goes when LOG_S is not a multiple of 4:
+// 0 = the INTT's last level (and the NTT's first), 1 = the INTT's first level
+// (and the NTT's last). The autotuner chooses per side.
+template <int LOG_S_, int SCHED_ = 0>
 struct ExtPlan {
     static constexpr int LOG_S = LOG_S_;
+    static constexpr int SCHED = SCHED_;
     static constexpr int S = 1 << LOG_S;
     static constexpr int NLEV = (LOG_S + 3) / 4;  // INTT levels (= NTT levels)
     static constexpr int EPT = LOG_S >= 4 ? 16 : S;
@@ -37,8 +41,11 @@ struct ExtPlan {
     static constexpr int Q4 = THREADS / TPQ;  // column quads per tile
     static constexpr int C = 4 * Q4;          // columns per tile
     static constexpr size_t SMEM = NLEV > 1 ? (size_t)S * Q4 * 16 : 0;
+    static constexpr int LEFT = LOG_S - 4 * (NLEV - 1);  // the leftover level's log2 radix
     // log2 radix of INTT level l; the NTT runs them in reverse order
-    __host__ __device__ static constexpr int lr(int l) { return l < NLEV - 1 ? 4 : LOG_S - 4 * (NLEV - 1); }
+    __host__ __device__ static constexpr int lr(int l) {
+        return SCHED == 0 ? (l < NLEV - 1 ? 4 : LEFT) : (l == 0 ? LEFT : 4);
+    }
     __host__ __device__ static constexpr int nlr(int l) { return lr(NLEV - 1 - l); }
     __host__ __device__ static constexpr int pre(int l) {
         int s = 0;
@@ -226,34 +233,57 @@ __device__ __forceinline__ void twist_and_first_ntt(V4* v, uint4* sm, int t, int
 
 // in: [S][cols] row-major, out: [2S][cols] row-major. cols % 4 == 0, 16-byte
 // aligned rows. Tiles of C columns are dealt to CTAs round-robin.
-template <int LOG_S>
+// Tiles a CTA visits: interleaved (tile = blockIdx.x + i * gridDim.x), or with
+// `blocked` one contiguous run of ceil(ntiles / gridDim.x) tiles per CTA.
+struct TileRange {
+    uint64_t first, last, step;
+    __device__ __forceinline__ TileRange(uint64_t ntiles, bool blocked) {
+        if (blocked) {
+            const uint64_t per = (ntiles + gridDim.x - 1) / gridDim.x;
+            first = blockIdx.x * per;
+            last = first + per < ntiles ? first + per : ntiles;
+            step = 1;
+        } else {
+            first = blockIdx.x;
+            last = ntiles;
+            step = gridDim.x;
+        }
+    }
+};
+
+template <int LOG_S, int SCHED = 0>
 __global__ void __launch_bounds__(512, 1)
     k_extend(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint64_t cols, uint64_t ntiles,
-             const Tw* __restrict__ tw, const Tw* __restrict__ twist_all) {
-    using PL = ExtPlan<LOG_S>;
+             const Tw* __restrict__ tw, const Tw* __restrict__ twist_all, uint32_t flags) {
+    using PL = ExtPlan<LOG_S, SCHED>;
     extern __shared__ uint4 sm[];
     const int tid = threadIdx.x;
     const int q = tid % PL::Q4;
     const int t = tid / PL::Q4;
     const Tw* twist = twist_all + PL::S;  // g^i / S for this side, i in [0, S)
     V4 v[PL::EPT];
-    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const TileRange tr(ntiles, flags & 1);
+    for (uint64_t tile = tr.first; tile < tr.last; tile += tr.step) {
         const uint64_t col = tile * PL::C + 4 * (uint64_t)q;
         const bool active = col < cols;
-        // INTT level 0 gathers rows t + L*n2 (L = S / R0) straight from HBM and
-        // writes them to the even output rows on the way.
+        // INTT level 0 gathers, for each of its G0 groups g, rows
+        // g*TPQ + t + L0*j (L0 = S / R0) straight from HBM and writes them to
+        // the even output rows on the way.
         constexpr int R0 = 1 << PL::lr(0);
+        constexpr int G0 = PL::EPT / R0;
         constexpr int L0 = PL::S / R0;
 #pragma unroll
-        for (int j = 0; j < R0; j++) {
-            const uint64_t row = (uint64_t)t + (uint64_t)L0 * j;
-            if (active) {
-                v[j] = ldg_stream_v4(in + row * cols + col);
-                stg_stream_v4(out + 2 * row * cols + col, v[j]);
-            } else {
-                v[j] = V4{{0, 0, 0, 0}};
+        for (int g = 0; g < G0; g++)
+#pragma unroll
+            for (int j = 0; j < R0; j++) {
+                const uint64_t row = (uint64_t)(g * PL::TPQ + t) + (uint64_t)L0 * j;
+                if (active) {
+                    v[g * R0 + j] = ldg_stream_v4(in + row * cols + col);
+                    stg_stream_v4(out + 2 * row * cols + col, v[g * R0 + j]);
+                } else {
+                    v[g * R0 + j] = V4{{0, 0, 0, 0}};
+                }
             }
-        }
         dif_levels<PL, 0, true>(v, sm, t, q, tw);
         twist_and_first_ntt<PL>(v, sm, t, q, tw, twist, out, cols, col, active);
     }

@@ -440,11 +440,13 @@ __device__ __forceinline__ int opaque(int x) {
 }
 
 // ---- one square ------------------------------------------------------------------
+// flags: bit 0 = blocked tile order (TileRange), bit 1 = no half-tile stagger
+// between the warp-groups.
 template <int LOG_S>
 __global__ void __launch_bounds__(512, 1)
     k_extend_tma(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_even,
                  uint32_t* __restrict__ out, uint64_t cols, uint64_t ntiles, const SideTables tb,
-                 int* __restrict__ err) {
+                 int* __restrict__ err, uint32_t flags) {
     using TP = TPlan<LOG_S>;
     extern __shared__ __align__(1024) unsigned char smem[];
     uint32_t* stage = reinterpret_cast<uint32_t*>(smem);
@@ -462,15 +464,17 @@ __global__ void __launch_bounds__(512, 1)
         fence_mbar_init();
     }
     __syncthreads();
-    uint64_t tile = blockIdx.x;
-    if (producer && tile < ntiles) tma_load_tile<TP>(stage, &tm_in, tile, full);
+    const TileRange tr(ntiles, flags & 1);
+    const bool stagger = !(flags & 2);
+    uint64_t tile = tr.first;
+    if (producer && tile < tr.last) tma_load_tile<TP>(stage, &tm_in, tile, full);
     // Group 1 starts half a tile after group 0 so the two groups' barriers and
     // butterfly phases interleave; group 0 signals from the middle of its first tile.
-    if (grp == 1 && tile < ntiles) asm volatile("bar.sync 3, 512;" ::: "memory");
-    bool stagger_pending = grp == 0;
+    if (stagger && grp == 1 && tile < tr.last) asm volatile("bar.sync 3, 512;" ::: "memory");
+    bool stagger_pending = stagger && grp == 0 && tile < tr.last;
     V4 v[TP::EPT];
     uint32_t parity = 0;
-    for (; tile < ntiles; tile += gridDim.x, parity ^= 1) {
+    for (; tile < tr.last; tile += tr.step, parity ^= 1) {
         const int tid_l = opaque(tid);
         const Coords<TP> c(tid_l & 255, grp);
         uint2* xg = reinterpret_cast<uint2*>(smem + TP::OFF_X + (tid_l >> 8) * TP::X_BYTES);
@@ -487,8 +491,8 @@ __global__ void __launch_bounds__(512, 1)
         stage_read<TP>(v, smem, c);
         group_bar(bar);  // this group has copied the staging buffer out
         if ((tid & 255) == 0) mbar_arrive(empty);
-        const uint64_t next = tile + gridDim.x;
-        if (producer && next < ntiles) {
+        const uint64_t next = tile + tr.step;
+        if (producer && next < tr.last) {
             const bool e_ok = mbar_wait_bounded(empty, parity);  // the other group is done too
             bulk_wait_read0();  // the even-row store has finished reading staging
             fence_proxy_async();

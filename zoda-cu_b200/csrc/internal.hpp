@@ -53,6 +53,8 @@ struct zoda_ctx {
     zb::Tables tables;
     int* d_err = nullptr;  // device flag a kernel sets when a bounded wait gives up
     int impl = 0;          // zoda_extend_impl
+    zoda_plan plan[13] = {};  // per log2 side, valid where planned[] is set
+    bool planned[13] = {};
     // host-call staging: NHS streams, one input and one output buffer each, and
     // 4 timing events per chunk for up to MAX_CHUNKS chunks
     static constexpr int NHS = 3;
@@ -72,9 +74,19 @@ struct zoda_ctx {
 
 namespace zb {
 // Launches the fused extension kernel for side 2^log_s (0 <= log_s <= 12).
-// impl: 0 = automatic, 1 = direct-load kernel, 2 = TMA-staged kernel (sides 128..4096).
+// impl: 0 = the side's plan (tuned, or the default), 1 = direct-load kernel,
+// 2 = TMA-staged kernel (sides 32..4096), both with default knobs.
 zoda_status launch_extend(const zoda_ctx* ctx, int log_s, const uint32_t* in, uint32_t* out, uint64_t cols,
                           cudaStream_t st, int impl = 0);
+// The plan a side runs with impl 0 and no tuning.
+zoda_plan default_plan(int log_s);
+// ZODA_OK when the plan can run for this side.
+zoda_status check_plan(int log_s, const zoda_plan& p);
+// Launches one explicit plan.
+zoda_status launch_plan(const zoda_ctx* ctx, int log_s, const zoda_plan& p, const uint32_t* in, uint32_t* out,
+                        uint64_t cols, cudaStream_t st);
+// The L2 promotion a side's TMA loads use on this context (for the batch maps).
+int side_l2_promo(const zoda_ctx* ctx, int log_s);
 // Sets the dynamic shared memory attribute of every extension instantiation.
 zoda_status extend_init_attributes();
 // Frees what the general encode / decoder left in the context.

@@ -184,7 +184,9 @@ bool admit_and_launch(zoda_server* s, Slot& sl) {
         Request& r = s->reqs[id];
         zoda_square q{r.d_in, (uint32_t*)((char*)s->arena_mem.p + r.out_off), r.k, 0, r.cols};
         BatchSquare& b = sl.h_sq[n];
-        const zoda_status st = make_batch_square(q, &b);
+        int ls = 0;
+        while ((1u << ls) < r.k) ls++;
+        const zoda_status st = make_batch_square(q, &b, side_l2_promo(s->ctx, ls));
         r.t_launch = now;
         if (st != ZODA_OK) {
             r.state = RState::Done;

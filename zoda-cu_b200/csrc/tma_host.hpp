@@ -26,7 +26,8 @@ inline PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 // 2-D u32 tensor map: `rows` rows of `cols` elements, rows `row_bytes` apart,
 // boxes of box_r rows x box_c columns, zero fill out of bounds.
 inline zoda_status make_map(CUtensorMap* m, const void* base, uint64_t cols, uint64_t rows, uint64_t row_bytes,
-                            uint32_t box_c, uint32_t box_r, CUtensorMapSwizzle swz = CU_TENSOR_MAP_SWIZZLE_NONE) {
+                            uint32_t box_c, uint32_t box_r, CUtensorMapSwizzle swz = CU_TENSOR_MAP_SWIZZLE_NONE,
+                            int promo = 3) {
     auto fn = encode_fn();
     if (!fn) {
         set_last_error_text("cuTensorMapEncodeTiled unavailable");
@@ -37,7 +38,7 @@ inline zoda_status make_map(CUtensorMap* m, const void* base, uint64_t cols, uin
     const cuuint32_t box[2] = {box_c, box_r};
     const cuuint32_t estr[2] = {1, 1};
     CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, const_cast<void*>(base), dims, strides, box, estr,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, swz, (CUtensorMapL2promotion)promo,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         set_last_error_text("cuTensorMapEncodeTiled failed with CUresult " + std::to_string((int)r));
@@ -47,14 +48,15 @@ inline zoda_status make_map(CUtensorMap* m, const void* base, uint64_t cols, uin
 }
 
 // The input map and the even-output-row map of one square for side plan TP.
+// promo: L2 promotion of the input loads (0 none, 1 64 B, 2 128 B, 3 256 B).
 template <class TP>
 zoda_status make_tile_maps(CUtensorMap* m_in, CUtensorMap* m_even, const uint32_t* in, uint32_t* out,
-                           uint64_t cols) {
+                           uint64_t cols, int promo = 3) {
     const CUtensorMapSwizzle swz = TP::SWZ_MASK == 7   ? CU_TENSOR_MAP_SWIZZLE_128B
                                    : TP::SWZ_MASK == 3 ? CU_TENSOR_MAP_SWIZZLE_64B
                                    : TP::SWZ_MASK == 1 ? CU_TENSOR_MAP_SWIZZLE_32B
                                                        : CU_TENSOR_MAP_SWIZZLE_NONE;
-    zoda_status s = make_map(m_in, in, cols, TP::S, cols * 4, TP::BOX_C, TP::BOX_R, swz);
+    zoda_status s = make_map(m_in, in, cols, TP::S, cols * 4, TP::BOX_C, TP::BOX_R, swz, promo);
     if (s != ZODA_OK) return s;
     return make_map(m_even, out, cols, TP::S, cols * 8, TP::BOX_C, TP::BOX_R, swz);
 }
@@ -77,7 +79,7 @@ inline SideTables side_tables(const zoda_ctx* ctx, int log_s) {
 namespace zb {
 // Batch building blocks shared by zoda_batch_* and the serving loop (batch.cu).
 // Descriptor of one square; ZODA_ERR_UNSUPPORTED outside sides 32..2048.
-zoda_status make_batch_square(const zoda_square& q, BatchSquare* out);
+zoda_status make_batch_square(const zoda_square& q, BatchSquare* out, int promo = 3);
 // One launch of k_extend_batch over d_sq[0..nsq) (sorted by first), with
 // *d_counter already zero on `st`.
 zoda_status launch_batch_kernel(const zoda_ctx* ctx, const BatchSquare* d_sq, uint32_t nsq, uint64_t total_tiles,

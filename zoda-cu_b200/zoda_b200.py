@@ -15,6 +15,7 @@ every call here runs the CUDA kernels or raises.
 from __future__ import annotations
 
 import ctypes
+import json
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -35,7 +36,8 @@ EXPORTS = [
     "zoda_ntt_device_noalloc", "zoda_batch_create", "zoda_batch_run", "zoda_batch_elements",
     "zoda_batch_destroy", "zoda_server_create", "zoda_server_submit", "zoda_server_wait",
     "zoda_server_release", "zoda_server_cancel", "zoda_server_get_stats", "zoda_server_destroy",
-    "zoda_encode_device", "zoda_recover_device",
+    "zoda_encode_device", "zoda_recover_device", "zoda_autotune", "zoda_plan_get", "zoda_plan_set",
+    "zoda_plan_clear",
 ]
 
 _lib = None
@@ -72,6 +74,20 @@ class ZodaServerStats(ctypes.Structure):
 class ZodaTiming(ctypes.Structure):
     _fields_ = [("h2d_ms", ctypes.c_float), ("kernel_ms", ctypes.c_float),
                 ("d2h_ms", ctypes.c_float), ("total_ms", ctypes.c_float)]
+
+
+class ZodaPlan(ctypes.Structure):
+    """Per-side launch plan (include/zoda_b200.h, zoda_plan)."""
+    _fields_ = [("impl", ctypes.c_int32), ("sched", ctypes.c_int32), ("l2_promo", ctypes.c_int32),
+                ("blocked", ctypes.c_int32), ("stagger", ctypes.c_int32), ("ms", ctypes.c_float)]
+    KEYS = ("impl", "sched", "l2_promo", "blocked", "stagger", "ms")
+
+    def to_dict(self) -> dict:
+        return {k: (round(float(getattr(self, k)), 5) if k == "ms" else int(getattr(self, k))) for k in self.KEYS}
+
+    @classmethod
+    def from_dict(cls, d: dict) -> "ZodaPlan":
+        return cls(*[d.get(k, 0) for k in cls.KEYS])
 
 
 def load(path: str = LIB_PATH):
@@ -135,6 +151,15 @@ def load(path: str = LIB_PATH):
     L.zoda_recover_device.restype = ctypes.c_int
     L.zoda_recover_device.argtypes = [vp, vp, u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, vp,
                                       ctypes.POINTER(ctypes.c_uint64), vp]
+    L.zoda_autotune.restype = ctypes.c_int
+    L.zoda_autotune.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32,
+                                ctypes.POINTER(ZodaPlan)]
+    L.zoda_plan_get.restype = ctypes.c_int
+    L.zoda_plan_get.argtypes = [vp, ctypes.c_uint32, ctypes.POINTER(ZodaPlan)]
+    L.zoda_plan_set.restype = ctypes.c_int
+    L.zoda_plan_set.argtypes = [vp, ctypes.c_uint32, ctypes.POINTER(ZodaPlan)]
+    L.zoda_plan_clear.restype = None
+    L.zoda_plan_clear.argtypes = [vp]
     L.zoda_ntt_device_noalloc.restype = ctypes.c_int
     L.zoda_ntt_device_noalloc.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, vp]
     L.zoda_extend_host.restype = ctypes.c_int
@@ -214,6 +239,49 @@ class Context:
                                           ctypes.byref(mm) if check else None, _stream_handle(stream)),
                "zoda_recover_device")
         return int(mm.value) if check else None
+
+    def autotune(self, side_min: int, side_max: int, cols: int = 0, reps: int = 5) -> dict:
+        """Tune every power-of-two side in [side_min, side_max]; returns {side: plan dict}
+        and installs the chosen plans on this context."""
+        arr = (ZodaPlan * 13)()
+        _check(load().zoda_autotune(self._h, side_min, side_max, cols, reps, arr), "zoda_autotune")
+        out, s = {}, side_min
+        while s <= side_max:
+            out[s] = arr[s.bit_length() - 1].to_dict()
+            s *= 2
+        return out
+
+    def plan_get(self, side: int):
+        """The side's installed plan as a dict, or None when it has none."""
+        p = ZodaPlan()
+        st = load().zoda_plan_get(self._h, side, ctypes.byref(p))
+        if st == 8:  # ZODA_ERR_STATE: no plan
+            return None
+        _check(st, "zoda_plan_get")
+        return p.to_dict()
+
+    def plan_set(self, side: int, plan: dict):
+        p = ZodaPlan.from_dict(plan)
+        _check(load().zoda_plan_set(self._h, side, ctypes.byref(p)), "zoda_plan_set")
+
+    def plan_clear(self):
+        load().zoda_plan_clear(self._h)
+
+    def save_plans(self, path: str):
+        """Write every installed plan as JSON {side: plan} (a tuning cache)."""
+        plans = {}
+        for ls in range(13):
+            p = self.plan_get(1 << ls)
+            if p is not None:
+                plans[str(1 << ls)] = p
+        with open(path, "w") as f:
+            json.dump(plans, f, indent=1, sort_keys=True)
+
+    def load_plans(self, path: str):
+        with open(path) as f:
+            plans = json.load(f)
+        for side, p in plans.items():
+            self.plan_set(int(side), p)
 
     def set_impl(self, impl: int):
         """0 = automatic, 1 = direct-load kernel, 2 = TMA-staged kernel."""
