@@ -207,10 +207,73 @@ def run_reference(args, world, rank):
 # our arm
 # ---------------------------------------------------------------------------
 
-def kernel_name(side: int) -> str:
-    """The kernel zoda_extend_device launches for this side (automatic variant)."""
+def kernel_name(side: int, plan: dict | None = None) -> str:
+    """The kernel zoda_extend_device launches for this side under `plan` (default plan if None)."""
     ls = side.bit_length() - 1
-    return f"k_extend_tma<{ls}>" if 7 <= ls <= 11 else f"k_extend<{ls}>"
+    tma = plan["impl"] == 2 if plan else 7 <= ls <= 11
+    if tma:
+        return f"k_extend_tma<{ls}>"
+    return f"k_extend<{ls},{plan['sched'] if plan else 0}>"
+
+
+def tune(ctx, side: int, cols: int, reps: int = 3) -> dict:
+    """Autotune one side at the workload's own column count (zoda_autotune) and return the plan it installed."""
+    return ctx.autotune(side, side, cols, reps)[side]
+
+
+def time_recover(ctx, k: int, reps: int = 5, seed: int = 3) -> dict:
+    """k-of-2k erasure recovery (zoda_recover_device) of a [2k][128k] extension with a seeded random half of
+    the rows erased, device-resident; payload = the recovered k x k square of 512-byte shares."""
+    import torch
+    import numpy as np
+    cols = k * SHARE_U32
+    gen = torch.Generator(device="cuda").manual_seed(4321)
+    d_in = torch.randint(0, P, (k, cols), dtype=torch.int64, device="cuda", generator=gen).to(torch.int32)
+    code = torch.empty((2 * k, cols), dtype=torch.int32, device="cuda")
+    ctx.extend(d_in, code, k, cols)
+    known = np.sort(np.random.default_rng(seed).choice(2 * k, size=k, replace=False))
+    out = torch.empty((k, cols), dtype=torch.int32, device="cuda")
+    ctx.recover(code, known, k, cols, out)
+    torch.cuda.synchronize()
+    ok = bool(torch.equal(out, d_in))
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(reps):
+        ctx.recover(code, known, k, cols, out, stream=stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / reps
+    del d_in, code, out
+    torch.cuda.empty_cache()
+    return {"k": k, "cols": cols, "erased_rows": k, "ms": round(ms, 4),
+            "gbps": round(payload_bits(k) / (ms * 1e-3) / 1e9, 1), "bit_exact": ok,
+            "api": "zoda_recover_device (4 column transforms over 2k points)"}
+
+
+def time_encode_general(ctx, k: int, n: int, reps: int = 5) -> dict:
+    """Encode of a non-power-of-two shape (zoda_encode_device): [k][128k] -> [k+n][128k], device-resident."""
+    import torch
+    cols = k * SHARE_U32
+    gen = torch.Generator(device="cuda").manual_seed(77)
+    d_in = torch.randint(0, P, (k, cols), dtype=torch.int64, device="cuda", generator=gen).to(torch.int32)
+    d_out = torch.empty((k + n, cols), dtype=torch.int32, device="cuda")
+    ctx.encode(d_in, d_out, k, n, cols)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(reps):
+        ctx.encode(d_in, d_out, k, n, cols, stream=stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / reps
+    ok = bool(torch.equal(d_out[0::2][:k // 2 + 1, :256], d_in[:k // 2 + 1, :256]))  # data rows at even rows
+    del d_in, d_out
+    torch.cuda.empty_cache()
+    return {"k": k, "n": n, "cols": cols, "ms": round(ms, 4),
+            "gbps": round(k * k * 512 * 8.0 / (ms * 1e-3) / 1e9, 1), "data_rows_ok": ok,
+            "api": "zoda_encode_device (interpolate over next_pow2(k), one evaluation per coset)"}
 
 
 def time_device_extend(ctx, side: int, steps: int, warmup: int, world: int, sampler=None):
@@ -444,6 +507,7 @@ def run_ours(args, world, rank, local):
     ctx = zoda_b200.Context(local)
     side = args.side
     cols = side * SHARE_U32
+    plan = None if args.no_tune else tune(ctx, side, cols)
     sampler = ClockSampler(local) if rank == 0 else None
     ms, clocks = time_device_extend(ctx, side, args.steps, args.warmup, world, sampler)
     ms_max = max_over_ranks(ms, world)
@@ -467,15 +531,21 @@ def run_ours(args, world, rank, local):
         for s2 in args.extra_sides:
             if s2 == side:
                 continue
+            plan2 = None if args.no_tune else tune(ctx, s2, s2 * SHARE_U32)
             ms2, _ = time_device_extend(ctx, s2, max(3, args.steps // 2), 3, 1)
             t2 = ms2 / max(3, args.steps // 2)
             extra[f"side{s2}"] = {
                 "ms_per_step": round(t2, 4), "gbps": round(payload_bits(s2) / (t2 * 1e-3) / 1e9, 1),
-                "hbm_frac": round(12.0 * s2 * s2 * SHARE_U32 / (t2 * 1e-3) / 1e9 / peaks["hbm_gbs"], 4)}
+                "hbm_frac": round(12.0 * s2 * s2 * SHARE_U32 / (t2 * 1e-3) / 1e9 / peaks["hbm_gbs"], 4),
+                "kernel": kernel_name(s2, plan2), "plan": plan2}
+        extra["recover_k1024"] = time_recover(ctx, 1024)
+        extra["encode_k1000_n1000"] = time_encode_general(ctx, 1000, 1000)
         refc = time_reference_cuda(min(side, 1024))
         if refc:
             extra["reference_cuda_kernel"] = refc
         if not args.no_batch:
+            if not args.no_tune:  # the batch's smaller sides (the larger ones were tuned above)
+                ctx.autotune(32, 512, 0, 3)
             extra["batched_mixed_squares"] = time_batched(ctx, args.batch_squares)
             extra["serving"] = time_serving(ctx, args.serve_rate, args.serve_requests)
     if rank == 0:
@@ -491,10 +561,11 @@ def run_ours(args, world, rank, local):
             "config": {"workload": f"plain device-resident extension of one {side}x{side} square per GPU "
                                    f"([{side}][{cols}] u32 -> [{2 * side}][{cols}])",
                        "side": side, "cols": cols, "share_bytes": 512,
+                       "plan": plan, "plan_source": "zoda_autotune at this workload" if plan else "default",
                        "l2": "inputs (and outputs) larger than the 126 MB L2; no flush"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
-                         "peak_source": peaks["source"], "kernel": kernel_name(side),
+                         "peak_source": peaks["source"], "kernel": kernel_name(side, plan),
                          "alg_bytes_per_launch": alg_bytes},
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -519,6 +590,7 @@ def main():
     ap.add_argument("--extra-sides", type=int, nargs="*", default=[2048, 4096])
     ap.add_argument("--no-extra", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched and serving report lines")
+    ap.add_argument("--no-tune", action="store_true", help="run the default plans instead of tuning first")
     ap.add_argument("--batch-squares", type=int, default=96)
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-requests", type=int, default=1000)
