@@ -302,6 +302,38 @@ zoda_status zoda_encode_device(zoda_ctx* ctx, const uint32_t* d_in, uint32_t* d_
 zoda_status zoda_recover_device(zoda_ctx* ctx, const uint32_t* d_code, const uint32_t* known_rows, uint32_t nknown,
                                 uint32_t k, uint64_t cols, uint32_t* d_data, uint64_t* mismatch, void* stream);
 
+/* ----------------------------------------------------------------------
+ * Row-side consumers: data root and random linear combinations
+ * ---------------------------------------------------------------------- */
+
+/* compute_data_root (src/benchmarks/utils.rs:51-59): SHA-256 over the
+ * little-endian bytes of rows[0 .. nrows*cols) (row-major, host memory),
+ * written as 64 lowercase hex digits plus a NUL. Host only, no GPU needed. */
+zoda_status zoda_data_root_host(const uint32_t* rows, uint64_t nrows, uint64_t cols, char out_hex[65]);
+
+/* generate_deterministic_coefficients (src/zoda/rlc.rs:48-65) on the device:
+ * for column i < ncols, digest = SHA-256(root[0 .. root_len) || u64_le(i)) and
+ * d_coeff[4*i + l] = u64_be(digest[8l .. 8l+8)) mod p, l < 4 (RLC_LIMBS,
+ * rlc.rs:18). `root` is the hex string of the data root. Asynchronous. */
+zoda_status zoda_rlc_coefficients_device(zoda_ctx* ctx, const char* root, size_t root_len, uint64_t ncols,
+                                         uint32_t* d_coeff, void* stream);
+
+/* rlc_row (src/zoda/rlc.rs:32-40) for every row: d_out[4*r + l] =
+ * sum_c d_rows[r*cols + c] * d_coeff[4*c + l] mod p, rows < 524288.
+ * One HBM read of the matrix. Asynchronous. */
+zoda_status zoda_rlc_rows_device(zoda_ctx* ctx, const uint32_t* d_rows, uint32_t rows, uint64_t cols,
+                                 const uint32_t* d_coeff, uint32_t* d_out, void* stream);
+
+/* The RLC soundness check of src/benchmarks/utils.rs:225-272 over EVERY
+ * encoded row instead of 64 samples: the RLC of the k data rows d_data
+ * [k][cols], extended like the data (zoda_encode_device with cols = 4), must
+ * equal the RLC of each of the k + n encoded rows d_code [k+n][cols], limb
+ * for limb. Stores the number of (row, limb) pairs that differ in
+ * *mismatches (0 = the encoding passes) and synchronizes `stream`. */
+zoda_status zoda_rlc_check_device(zoda_ctx* ctx, const uint32_t* d_data, const uint32_t* d_code, uint32_t k,
+                                  uint32_t n, uint64_t cols, const uint32_t* d_coeff, uint64_t* mismatches,
+                                  void* stream);
+
 /* ======================================================================
  * Part 3: a transform for callers that cannot allocate device memory
  * ====================================================================== */

@@ -229,6 +229,7 @@ void zoda_ctx_destroy(zoda_ctx* c) {
         for (auto& e : row)
             if (e) cudaEventDestroy(e);
     general_release(c);
+    rlc_release(c);
     if (c->d_err) cudaFree(c->d_err);
     if (c->tables.tw) cudaFree(c->tables.tw);
     if (c->tables.twist) cudaFree(c->tables.twist);

@@ -37,7 +37,8 @@ EXPORTS = [
     "zoda_batch_destroy", "zoda_server_create", "zoda_server_submit", "zoda_server_wait",
     "zoda_server_release", "zoda_server_cancel", "zoda_server_get_stats", "zoda_server_destroy",
     "zoda_encode_device", "zoda_recover_device", "zoda_autotune", "zoda_plan_get", "zoda_plan_set",
-    "zoda_plan_clear",
+    "zoda_plan_clear", "zoda_data_root_host", "zoda_rlc_coefficients_device", "zoda_rlc_rows_device",
+    "zoda_rlc_check_device",
 ]
 
 _lib = None
@@ -160,6 +161,15 @@ def load(path: str = LIB_PATH):
     L.zoda_plan_set.argtypes = [vp, ctypes.c_uint32, ctypes.POINTER(ZodaPlan)]
     L.zoda_plan_clear.restype = None
     L.zoda_plan_clear.argtypes = [vp]
+    L.zoda_data_root_host.restype = ctypes.c_int
+    L.zoda_data_root_host.argtypes = [vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_char_p]
+    L.zoda_rlc_coefficients_device.restype = ctypes.c_int
+    L.zoda_rlc_coefficients_device.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_uint64, vp, vp]
+    L.zoda_rlc_rows_device.restype = ctypes.c_int
+    L.zoda_rlc_rows_device.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_uint64, vp, vp, vp]
+    L.zoda_rlc_check_device.restype = ctypes.c_int
+    L.zoda_rlc_check_device.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, vp,
+                                        ctypes.POINTER(ctypes.c_uint64), vp]
     L.zoda_ntt_device_noalloc.restype = ctypes.c_int
     L.zoda_ntt_device_noalloc.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, vp]
     L.zoda_extend_host.restype = ctypes.c_int
@@ -240,6 +250,25 @@ class Context:
                "zoda_recover_device")
         return int(mm.value) if check else None
 
+    def rlc_coefficients(self, root: str, ncols: int, d_coeff, stream=None):
+        """src/zoda/rlc.rs:48-65 on the device: d_coeff [ncols][4] u32 from the data root's hex string."""
+        b = root.encode()
+        _check(load().zoda_rlc_coefficients_device(self._h, b, len(b), ncols, _addr(d_coeff),
+                                                   _stream_handle(stream)), "zoda_rlc_coefficients_device")
+
+    def rlc_rows(self, d_rows, rows: int, cols: int, d_coeff, d_out, stream=None):
+        """src/zoda/rlc.rs:32-40 for every row: d_out [rows][4]."""
+        _check(load().zoda_rlc_rows_device(self._h, _addr(d_rows), rows, cols, _addr(d_coeff), _addr(d_out),
+                                           _stream_handle(stream)), "zoda_rlc_rows_device")
+
+    def rlc_check(self, d_data, d_code, k: int, n: int, cols: int, d_coeff, stream=None) -> int:
+        """RLC check of every encoded row (src/benchmarks/utils.rs:225-272); returns the
+        number of mismatching (row, limb) pairs, 0 when the encoding passes."""
+        mm = ctypes.c_uint64(0)
+        _check(load().zoda_rlc_check_device(self._h, _addr(d_data), _addr(d_code), k, n, cols, _addr(d_coeff),
+                                            ctypes.byref(mm), _stream_handle(stream)), "zoda_rlc_check_device")
+        return int(mm.value)
+
     def autotune(self, side_min: int, side_max: int, cols: int = 0, reps: int = 5) -> dict:
         """Tune every power-of-two side in [side_min, side_max]; returns {side: plan dict}
         and installs the chosen plans on this context."""
@@ -296,6 +325,17 @@ class Context:
         _check(load().zoda_extend_host(self._h, _addr(h_in), _addr(h_out), k, cols, ctypes.byref(t)),
                "zoda_extend_host")
         return t
+
+
+def data_root(rows) -> str:
+    """compute_data_root (src/benchmarks/utils.rs:51-59) of a host row-major u32 array
+    (numpy), computed by the library's host SHA-256."""
+    import numpy as np
+    a = np.ascontiguousarray(rows, dtype=np.uint32)
+    out = ctypes.create_string_buffer(65)
+    nrows = a.shape[0] if a.ndim > 1 else 1
+    _check(load().zoda_data_root_host(a.ctypes.data, nrows, a.size // max(1, nrows), out), "zoda_data_root_host")
+    return out.value.decode()
 
 
 def _stream_handle(stream):
