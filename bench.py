@@ -251,6 +251,47 @@ def time_recover(ctx, k: int, reps: int = 5, seed: int = 3) -> dict:
             "api": "zoda_recover_device (4 column transforms over 2k points)"}
 
 
+def time_rlc(ctx, k: int, reps: int = 5) -> dict:
+    """RLC consumers on the k x k extension (k x 128k data, 2k x 128k code): coefficients from a data
+    root (device SHA-256 per column), RLC of every code row, and the full check of every row."""
+    import torch
+    cols = k * SHARE_U32
+    gen = torch.Generator(device="cuda").manual_seed(11)
+    d_in = torch.randint(0, P, (k, cols), dtype=torch.int64, device="cuda", generator=gen).to(torch.int32)
+    code = torch.empty((2 * k, cols), dtype=torch.int32, device="cuda")
+    ctx.extend(d_in, code, k, cols)
+    coeff = torch.empty((cols, 4), dtype=torch.int32, device="cuda")
+    rl = torch.empty((2 * k, 4), dtype=torch.int32, device="cuda")
+    root = "ab" * 32  # any 64-hex-digit root: hashing the whole square is a host step, timed separately below
+    stream = torch.cuda.current_stream()
+    ctx.rlc_coefficients(root, cols, coeff)
+    ctx.rlc_rows(code, 2 * k, cols, coeff, rl)
+    mm = ctx.rlc_check(d_in, code, k, k, cols, coeff)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev[0].record(stream)
+    for _ in range(reps):
+        ctx.rlc_coefficients(root, cols, coeff, stream=stream)
+    ev[1].record(stream)
+    for _ in range(reps):
+        ctx.rlc_rows(code, 2 * k, cols, coeff, rl, stream=stream)
+    ev[2].record(stream)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        mm |= ctx.rlc_check(d_in, code, k, k, cols, coeff, stream=stream)
+    t_check = (time.perf_counter() - t0) * 1e3 / reps
+    coeff_ms = ev[0].elapsed_time(ev[1]) / reps
+    rows_ms = ev[1].elapsed_time(ev[2]) / reps
+    code_bytes = 2 * k * cols * 4
+    del d_in, code
+    torch.cuda.empty_cache()
+    return {"k": k, "cols": cols, "coefficients_ms": round(coeff_ms, 4), "rlc_code_rows_ms": round(rows_ms, 4),
+            "rlc_code_rows_gbs": round(code_bytes / (rows_ms * 1e-3) / 1e9, 1),
+            "rlc_code_rows_hbm_frac": round(code_bytes / (rows_ms * 1e-3) / 1e9 / measured_peaks()["hbm_gbs"], 4),
+            "check_all_rows_ms": round(t_check, 3), "check_mismatches": mm,
+            "api": "zoda_rlc_coefficients_device, zoda_rlc_rows_device, zoda_rlc_check_device (synchronous)"}
+
+
 def time_encode_general(ctx, k: int, n: int, reps: int = 5) -> dict:
     """Encode of a non-power-of-two shape (zoda_encode_device): [k][128k] -> [k+n][128k], device-resident."""
     import torch
@@ -377,12 +418,12 @@ def log_uniform_sides(n: int, lo: int, hi: int, seed: int):
     return [1 << int(rng.integers(lo.bit_length() - 1, hi.bit_length())) for _ in range(n)]
 
 
-def time_batched(ctx, n: int) -> dict:
-    """n squares, sides log-uniform over 32..2048 (seed 0), 128 u32 per share: one batched
+def time_batched(ctx, n: int, hi: int = 2048) -> dict:
+    """n squares, sides log-uniform over 32..hi (seed 0), 128 u32 per share: one batched
     persistent launch (graph replay) against plain calls, one square at a time."""
     import torch
     import zoda_b200
-    sides = log_uniform_sides(n, 32, 2048, seed=0)
+    sides = log_uniform_sides(n, 32, hi, seed=0)
     sq = []
     for s in sides:
         a = torch.randint(0, P, (s, s * SHARE_U32), dtype=torch.int64, device="cuda").to(torch.int32)
@@ -540,6 +581,7 @@ def run_ours(args, world, rank, local):
                 "kernel": kernel_name(s2, plan2), "plan": plan2}
         extra["recover_k1024"] = time_recover(ctx, 1024)
         extra["encode_k1000_n1000"] = time_encode_general(ctx, 1000, 1000)
+        extra["rlc_k1024"] = time_rlc(ctx, 1024)
         refc = time_reference_cuda(min(side, 1024))
         if refc:
             extra["reference_cuda_kernel"] = refc
@@ -547,6 +589,8 @@ def run_ours(args, world, rank, local):
             if not args.no_tune:  # the batch's smaller sides (the larger ones were tuned above)
                 ctx.autotune(32, 512, 0, 3)
             extra["batched_mixed_squares"] = time_batched(ctx, args.batch_squares)
+            # where launch overhead dominates: the same draw restricted to sides 32..256
+            extra["batched_small_squares"] = time_batched(ctx, args.batch_squares, hi=256)
             extra["serving"] = time_serving(ctx, args.serve_rate, args.serve_requests)
     if rank == 0:
         cpu = cpu_port_rate(side, args.cpu_budget)
