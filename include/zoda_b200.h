@@ -87,10 +87,9 @@ void zoda_ctx_destroy(zoda_ctx* ctx);
 /* Largest k the fused extension accepts (4096). */
 uint32_t zoda_max_side(void);
 
-/* Kernel variant of the fused extension on a context. AUTO picks the
- * TMA-staged kernel for 128 <= k <= 2048 and the direct-load kernel
- * otherwise; the others force one (for tests and tuning; TMA supports k in
- * [128, 4096]). */
+/* Kernel variant of the fused extension on a context. AUTO runs the side's
+ * plan (below); the others force one kernel with default knobs (for tests;
+ * TMA supports k in [32, 4096]). */
 typedef enum zoda_extend_impl {
     ZODA_IMPL_AUTO = 0,
     ZODA_IMPL_DIRECT = 1,
@@ -111,7 +110,9 @@ typedef struct zoda_plan {
     int32_t l2_promo; /* TMA kernel: L2 promotion of tile loads, 0 none, 1 64 B,
                          2 128 B, 3 256 B                                              */
     int32_t blocked;  /* 0 = CTA i takes tiles i, i + grid, ...; 1 = one contiguous run */
-    int32_t stagger;  /* TMA kernel: 1 = the two warp-groups run half a tile apart     */
+    int32_t stagger;  /* TMA kernel: 0 = the two warp-groups run in step; 1, 2, 3 = the
+                         second starts once the first begins its last INTT level, its
+                         second INTT level, or its first (less apart, more shared code) */
     float ms;         /* the tuner's time for this plan (0 when set by hand)            */
 } zoda_plan;
 

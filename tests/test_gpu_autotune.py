@@ -52,7 +52,7 @@ def plans_for(side: int):
             out.append(dict(impl=1, sched=sched, l2_promo=3, blocked=blocked, stagger=1))
         if ls >= 5:
             for promo in (3, 2, 0):
-                for stagger in (1, 0):
+                for stagger in (1, 2, 3, 0):
                     out.append(dict(impl=2, sched=0, l2_promo=promo, blocked=blocked, stagger=stagger))
     return out
 

@@ -10,7 +10,8 @@
 //
 // Candidates: the direct-load kernel with either radix schedule and either
 // tile order; the TMA-staged kernel (sides >= 32) with L2 promotion 256 B,
-// 128 B or none, either tile order, with and without the warp-group stagger.
+// 128 B or none, either tile order, and the warp-group stagger at each of its
+// three release points or off.
 #include <algorithm>
 #include <vector>
 
@@ -72,7 +73,7 @@ std::vector<zoda_plan> candidates(int ls) {
         }
         if (ls >= 5)
             for (int promo : {3, 2, 0})
-                for (int stagger = 1; stagger >= 0; stagger--) {
+                for (int stagger : {1, 2, 3, 0}) {
                     zoda_plan p = d;
                     p.impl = ZODA_IMPL_TMA;
                     p.sched = 0;

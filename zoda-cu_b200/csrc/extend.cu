@@ -103,7 +103,7 @@ zoda_status check_plan(int log_s, const zoda_plan& p) {
     if (p.impl != ZODA_IMPL_DIRECT && p.impl != ZODA_IMPL_TMA) return ZODA_ERR_ARG;
     if (p.impl == ZODA_IMPL_TMA && log_s < 5) return ZODA_ERR_UNSUPPORTED;
     if (p.sched < 0 || p.sched > 1 || p.l2_promo < 0 || p.l2_promo > 3 || p.blocked < 0 || p.blocked > 1 ||
-        p.stagger < 0 || p.stagger > 1)
+        p.stagger < 0 || p.stagger > 3)
         return ZODA_ERR_ARG;
     return ZODA_OK;
 }
@@ -118,7 +118,9 @@ zoda_status launch_plan(const zoda_ctx* ctx, int log_s, const zoda_plan& p, cons
                         uint64_t cols, cudaStream_t st) {
     zoda_status s = check_plan(log_s, p);
     if (s != ZODA_OK) return s;
-    const uint32_t flags = (p.blocked ? 1u : 0u) | (p.stagger ? 0u : 2u);
+    // stagger 1: release after all INTT levels but the last; 2: after the first; 3: right away
+    const uint32_t at_code = p.stagger == 2 ? 2u : p.stagger == 3 ? 1u : 0u;
+    const uint32_t flags = (p.blocked ? 1u : 0u) | (p.stagger ? 0u : 2u) | (at_code << 2);
     if (p.impl == ZODA_IMPL_TMA) {
         switch (log_s) {
 #define ZB_CASE(L) \

@@ -293,9 +293,19 @@ __device__ __forceinline__ void exchange(V4* v, uint2* xg, int ql, int bar, cons
 
 // INTT levels l .. NLEV-2 (each followed by an exchange); the last INTT level is
 // run by the kernel body.
+// With stagger_pending set, group 0 releases group 1 (named barrier 3) as it
+// starts INTT level `stagger_at`.
+__device__ __forceinline__ void stagger_release(bool& stagger_pending) {
+    if (stagger_pending) {
+        asm volatile("bar.arrive 3, 512;" ::: "memory");
+        stagger_pending = false;
+    }
+}
 template <class TP, int l>
-__device__ __forceinline__ void intt_upto_last(V4* v, uint2* xg, int t, int ql, int bar, const SideTables& tb) {
+__device__ __forceinline__ void intt_upto_last(V4* v, uint2* xg, int t, int ql, int bar, const SideTables& tb,
+                                               bool& stagger_pending, int stagger_at) {
     if constexpr (l < TP::NLEV - 1) {
+        if (l == stagger_at) stagger_release(stagger_pending);
         using W = LvlGeom<TP, TP::lr(l), TP::pre(l)>;
         using Rd = LvlGeom<TP, TP::lr(l + 1), TP::pre(l + 1)>;
 #pragma unroll
@@ -306,7 +316,7 @@ __device__ __forceinline__ void intt_upto_last(V4* v, uint2* xg, int t, int ql, 
         exchange<TP, W::R, W::LOGL, Rd::R, Rd::LOGL>(
             v, xg, ql, bar, [&](int g) { return W::base(W::gid(g, t)); },
             [&](int g) { return Rd::base(Rd::gid(g, t)); });
-        intt_upto_last<TP, l + 1>(v, xg, t, ql, bar, tb);
+        intt_upto_last<TP, l + 1>(v, xg, t, ql, bar, tb, stagger_pending, stagger_at);
     }
 }
 
@@ -386,19 +396,16 @@ __device__ __forceinline__ void stage_read(V4* v, const unsigned char* smem, con
 }
 
 // Everything after the tile is in registers: INTT, twist, NTT, odd-row stores.
-// With stagger_pending set, group 0 releases group 1 (named barrier 3) from the
-// middle of the tile.
+// With stagger_pending set, group 0 releases group 1 (named barrier 3) when it
+// starts INTT level stagger_at (NLEV-1: after all INTT levels but the last).
 template <class TP>
 __device__ __forceinline__ void tile_compute(V4* v, uint2* xg, const Coords<TP>& c, int bar, const SideTables& tb,
                                              uint32_t* __restrict__ out, uint64_t cols, uint64_t col, bool active,
-                                             bool& stagger_pending) {
+                                             bool& stagger_pending, int stagger_at = TP::NLEV - 1) {
     const int t = c.t, ql = c.ql;
     // ---- INTT levels 0 .. NLEV-2
-    intt_upto_last<TP, 0>(v, xg, t, ql, bar, tb);
-    if (stagger_pending) {
-        asm volatile("bar.arrive 3, 512;" ::: "memory");
-        stagger_pending = false;
-    }
+    intt_upto_last<TP, 0>(v, xg, t, ql, bar, tb, stagger_pending, stagger_at);
+    stagger_release(stagger_pending);
     {
         // ---- INTT last level (L = 1). Its outputs need the twist g^c / S with
         // c = c0 + k2*S/R; g^(k2*S/R) = omega_2R^k2 is an immediate folded into the
@@ -440,8 +447,9 @@ __device__ __forceinline__ int opaque(int x) {
 }
 
 // ---- one square ------------------------------------------------------------------
-// flags: bit 0 = blocked tile order (TileRange), bit 1 = no half-tile stagger
-// between the warp-groups.
+// flags: bit 0 = blocked tile order (TileRange), bit 1 = no stagger between the
+// warp-groups, bits 2-3 = the INTT level at which group 0 releases group 1,
+// plus one (0: the default, after all INTT levels but the last).
 template <int LOG_S>
 __global__ void __launch_bounds__(512, 1)
     k_extend_tma(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_even,
@@ -466,6 +474,7 @@ __global__ void __launch_bounds__(512, 1)
     __syncthreads();
     const TileRange tr(ntiles, flags & 1);
     const bool stagger = !(flags & 2);
+    const int stagger_at = (flags >> 2) & 3 ? (int)((flags >> 2) & 3) - 1 : TP::NLEV - 1;
     uint64_t tile = tr.first;
     if (producer && tile < tr.last) tma_load_tile<TP>(stage, &tm_in, tile, full);
     // Group 1 starts half a tile after group 0 so the two groups' barriers and
@@ -499,7 +508,7 @@ __global__ void __launch_bounds__(512, 1)
             if (e_ok) tma_load_tile<TP>(stage, &tm_in, next, full);
             else atomicOr(err, 2);  // both groups then time out on `full` and leave
         }
-        tile_compute<TP>(v, xg, c, bar, tb, out, cols, col, active, stagger_pending);
+        tile_compute<TP>(v, xg, c, bar, tb, out, cols, col, active, stagger_pending, stagger_at);
     }
     if (stagger_pending) asm volatile("bar.arrive 3, 512;" ::: "memory");
     if (producer) bulk_wait0();
