@@ -129,14 +129,21 @@ def dist_setup():
     return world, rank, local
 
 
-def max_over_ranks(x: float, world: int) -> float:
+def max_over_ranks(x: float, world: int, device: str = "cuda") -> float:
+    """The slowest rank's value (every rank gets it). NCCL needs a CUDA tensor; gloo takes CPU."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_rate(world: int, side: int, ms_max: float, steps: int) -> float:
+    """Whole-job payload Gb/s: every rank encodes one side x side square per step (weak scaling),
+    timed by the slowest rank."""
+    return world * payload_bits(side) / (ms_max / steps * 1e-3) / 1e9
 
 
 def barrier(world: int):
@@ -180,7 +187,7 @@ def run_reference(args, world, rank):
         return
     side = args.side
     rates = []
-    per_step_budget = max(2.0, min(20.0, 60.0 / max(1, args.steps + args.warmup)))
+    per_step_budget = args.ref_step_budget or max(2.0, min(20.0, 60.0 / max(1, args.steps + args.warmup)))
     for i in range(args.warmup + args.steps):
         r = cpu_port_rate(side, per_step_budget, seed=1 + i)
         if i >= args.warmup:
@@ -553,7 +560,7 @@ def run_ours(args, world, rank, local):
     ms, clocks = time_device_extend(ctx, side, args.steps, args.warmup, world, sampler)
     ms_max = max_over_ranks(ms, world)
     t_step = ms_max / args.steps
-    value = world * payload_bits(side) / (t_step * 1e-3) / 1e9
+    value = job_rate(world, side, ms_max, args.steps)
     alg_bytes = 12.0 * side * cols  # read [side][cols] + write [2 side][cols] u32
     peaks = measured_peaks()
     achieved = alg_bytes / (ms / args.steps * 1e-3) / 1e9
@@ -639,6 +646,8 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-requests", type=int, default=1000)
     ap.add_argument("--cpu-budget", type=float, default=10.0, help="seconds of CPU baseline sampling")
+    ap.add_argument("--ref-step-budget", type=float, default=None,
+                    help="seconds of CPU work per step of --impl reference (default: about 60 s in total)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps
     world, rank, local = dist_setup()
