@@ -294,7 +294,7 @@ zoda_status zoda_encode_device(zoda_ctx* ctx, const uint32_t* d_in, uint32_t* d_
  * zoda_extend_device writes them); only the rows listed in known_rows[0 ..
  * nknown) are read, the others may hold anything. At least k distinct rows
  * must be known. d_data receives the original [k][cols] data. k is a power of
- * two <= 2048. When every even row is known the data is copied out; otherwise
+ * two <= 4096. When every even row is known the data is copied out; otherwise
  * the call runs four column transforms over 2k points (see general.cu) with
  * the context's scratch (<= 512 MiB). If `mismatch` is not NULL the call also
  * checks that the known rows are one codeword, stores the number of

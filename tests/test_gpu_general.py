@@ -121,9 +121,9 @@ def recover(ctx, code, known, k, cols, check=False):
     return from_dev(out), mm
 
 
-@pytest.mark.parametrize("k", [1, 2, 4, 16, 64, 256, 1024, 2048])
+@pytest.mark.parametrize("k", [1, 2, 4, 16, 64, 256, 1024, 2048, 4096])
 def test_recover_random_k_of_2k(ctx, k):
-    cols = 4096 + 36 if k <= 256 else (260 if k == 1024 else 132)
+    cols = 4096 + 36 if k <= 256 else {1024: 260, 2048: 132, 4096: 20}[k]
     data = O.seeded_input(k, cols, seed=500 + k)
     code = encoded(ctx, data)
     rng = np.random.default_rng(k)
@@ -200,4 +200,4 @@ def test_recover_bad_args(ctx):
         ctx.recover(code, range(k), 12, cols, out)              # k not a power of two
     big = torch.zeros((8, 8), dtype=torch.int32, device="cuda")
     with pytest.raises(zoda_b200.ZodaError):
-        ctx.recover(big, range(4096), 4096, 8, big)             # beyond k = 2048
+        ctx.recover(big, range(8192), 8192, 8, big)             # beyond k = 4096

@@ -57,13 +57,13 @@ zoda_status coltx_t(const zoda_ctx* ctx, const ColTx& a, cudaStream_t st) {
     return ZODA_OK;
 }
 
-// Column transform of size 2^log_n (1 <= log_n <= 12).
+// Column transform of size 2^log_n (1 <= log_n <= 13).
 zoda_status coltx(const zoda_ctx* ctx, int log_n, bool inv, const ColTx& a, cudaStream_t st) {
     switch (log_n) {
 #define ZB_CASE(L) \
     case L: return inv ? coltx_t<L, true>(ctx, a, st) : coltx_t<L, false>(ctx, a, st);
         ZB_CASE(1) ZB_CASE(2) ZB_CASE(3) ZB_CASE(4) ZB_CASE(5) ZB_CASE(6)
-        ZB_CASE(7) ZB_CASE(8) ZB_CASE(9) ZB_CASE(10) ZB_CASE(11) ZB_CASE(12)
+        ZB_CASE(7) ZB_CASE(8) ZB_CASE(9) ZB_CASE(10) ZB_CASE(11) ZB_CASE(12) ZB_CASE(13)
 #undef ZB_CASE
         default: return ZODA_ERR_UNSUPPORTED;
     }
@@ -277,8 +277,8 @@ zoda_status zoda_recover_device(zoda_ctx* ctx, const uint32_t* d_code, const uin
     if (((uintptr_t)d_code | (uintptr_t)d_data) & 15) return ZODA_ERR_ARG;
     const int lk = log2_exact64(k);
     if (lk < 0) return ZODA_ERR_ARG;
-    if (lk > 11) {
-        set_last_error_text("the decoder covers k <= 2048 (codewords of up to 4096 rows)");
+    if (lk > 12) {
+        set_last_error_text("the decoder covers k <= 4096 (codewords of up to 8192 rows)");
         return ZODA_ERR_UNSUPPORTED;
     }
     const uint32_t N = 2 * k;
