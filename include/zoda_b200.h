@@ -102,7 +102,8 @@ zoda_status zoda_ctx_set_impl(zoda_ctx* ctx, int impl);
  * ZODA_IMPL_AUTO a side that has a plan (from zoda_autotune or
  * zoda_plan_set) runs that plan; a side without one runs the default plan
  * (TMA for 128 <= k <= 2048, else direct; sched 0, l2_promo 3, blocked 0,
- * stagger 1). Every plan computes the same bits; only the speed differs. */
+ * stagger 1, radix 16). Every plan computes the same bits; only the speed
+ * differs. */
 typedef struct zoda_plan {
     int32_t impl;     /* ZODA_IMPL_DIRECT or ZODA_IMPL_TMA (k >= 32)                   */
     int32_t sched;    /* direct kernel: radix-16 levels with the leftover radix at the
@@ -113,6 +114,8 @@ typedef struct zoda_plan {
     int32_t stagger;  /* TMA kernel: 0 = the two warp-groups run in step; 1, 2, 3 = the
                          second starts once the first begins its last INTT level, its
                          second INTT level, or its first (less apart, more shared code) */
+    int32_t radix;    /* TMA kernel: level radix 16 (512 threads, 16 positions per
+                         thread) or 8 (1024 threads, 8 positions: twice the warps) */
     float ms;         /* the tuner's time for this plan (0 when set by hand)            */
 } zoda_plan;
 

@@ -51,9 +51,11 @@ def plans_for(side: int):
         for sched in ((0, 1) if ls >= 5 and ls % 4 else (0,)):
             out.append(dict(impl=1, sched=sched, l2_promo=3, blocked=blocked, stagger=1))
         if ls >= 5:
-            for promo in (3, 2, 0):
-                for stagger in (1, 2, 3, 0):
-                    out.append(dict(impl=2, sched=0, l2_promo=promo, blocked=blocked, stagger=stagger))
+            for radix in (16, 8):
+                for promo in (3, 2, 0):
+                    for stagger in (1, 2, 3, 0):
+                        out.append(dict(impl=2, sched=0, l2_promo=promo, blocked=blocked, stagger=stagger,
+                                        radix=radix))
     return out
 
 
@@ -112,6 +114,10 @@ def test_plan_errors(ctx):
         ctx.plan_set(64, dict(impl=2, sched=0, l2_promo=4, blocked=0, stagger=1))
     with pytest.raises(zoda_b200.ZodaError):
         ctx.plan_set(48, dict(impl=1, sched=0, l2_promo=3, blocked=0, stagger=1))  # not a power of two
+    with pytest.raises(zoda_b200.ZodaError):
+        ctx.plan_set(64, dict(impl=2, sched=0, l2_promo=3, blocked=0, stagger=1, radix=4))
+    with pytest.raises(zoda_b200.ZodaError):
+        ctx.plan_set(64, dict(impl=1, sched=0, l2_promo=3, blocked=0, stagger=1, radix=8))  # radix 8: TMA only
     with pytest.raises(zoda_b200.ZodaError):
         ctx.autotune(64, 32)
     assert ctx.plan_get(1024) is None

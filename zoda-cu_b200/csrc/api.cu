@@ -67,17 +67,19 @@ static void build_tables(std::vector<Tw>& tw, std::vector<Tw>& twist) {
 
 // Level tables of the TMA-staged kernel for side 2^ls (layout documented at
 // SideTables in extend_tma.cuh). Offsets are entries into `all`.
-static void build_side_tables(int ls, std::vector<Tw>& all, size_t off[5]) {
-    const int nlev = (ls + 3) / 4;
-    auto lr = [&](int l) { return l < nlev - 1 ? 4 : ls - 4 * (nlev - 1); };
+// Level tables of the TMA kernel for side 2^ls with level radix 2^lept
+// (off: INTT levels 0..2, NTT level 0 with the twist, NTT levels 1..2, end).
+static void build_side_tables(int ls, int lept, std::vector<Tw>& all, size_t off[8]) {
+    const int nlev = (ls + lept - 1) / lept;
+    auto lr = [&](int l) { return l < nlev - 1 ? lept : ls - lept * (nlev - 1); };
     auto nlr = [&](int l) { return lr(nlev - 1 - l); };
     const uint32_t S = 1u << ls;
     auto tw_of = [](uint32_t w) { return Tw{w, shoup(w)}; };
     auto pow_root = [](int logn, uint64_t e) { return powmod_c(root_of_unity(logn), e); };
-    for (int k = 0; k < 5; k++) off[k] = all.size();
+    for (int k = 0; k < 8; k++) off[k] = all.size();
     // INTT levels 0 .. nlev-2: [k2*L + m] = omega_N^(-m*k2)
     int pb = 0;
-    for (int l = 0; l < 2; l++) {
+    for (int l = 0; l < 3; l++) {
         off[l] = all.size();
         if (l < nlev - 1) {
             const int logn = ls - pb, R = 1 << lr(l), L = 1 << (logn - lr(l));
@@ -88,7 +90,7 @@ static void build_side_tables(int ls, std::vector<Tw>& all, size_t off[5]) {
         }
     }
     // NTT level 0 with the twist: [k2*NB + b] = g^c0 / S * omega_S^(c0*k2)
-    off[2] = all.size();
+    off[3] = all.size();
     {
         const int LR = lr(nlev - 1), R = 1 << LR;
         const uint32_t NB = S >> LR;
@@ -110,15 +112,17 @@ static void build_side_tables(int ls, std::vector<Tw>& all, size_t off[5]) {
     }
     // NTT levels 1 .. nlev-2: [k2*L + m] = omega_N^(m*k2)
     int npb = nlr(0);
-    off[3] = all.size();
-    if (nlev >= 3) {
-        const int l = 1;
-        const int logn = ls - npb, R = 1 << nlr(l), L = 1 << (logn - nlr(l));
-        const uint32_t N = 1u << logn;
-        for (int k2 = 0; k2 < R; k2++)
-            for (int m = 0; m < L; m++) all.push_back(tw_of(pow_root(logn, (uint64_t)m * k2 % N)));
+    for (int l = 1; l < 3; l++) {
+        off[3 + l] = all.size();
+        if (l <= nlev - 2) {
+            const int logn = ls - npb, R = 1 << nlr(l), L = 1 << (logn - nlr(l));
+            const uint32_t N = 1u << logn;
+            for (int k2 = 0; k2 < R; k2++)
+                for (int m = 0; m < L; m++) all.push_back(tw_of(pow_root(logn, (uint64_t)m * k2 % N)));
+            npb += nlr(l);
+        }
     }
-    off[4] = all.size();
+    off[6] = all.size();
 }
 
 static int log2_exact(uint64_t x) {
@@ -201,7 +205,8 @@ zoda_status zoda_ctx_create(int device, zoda_ctx** out) {
     }
     {
         std::vector<Tw> side;
-        for (int ls = 5; ls <= 12; ls++) build_side_tables(ls, side, c->tables.side_off[ls]);
+        for (int ls = 5; ls <= 12; ls++)
+            for (int r = 0; r < 2; r++) build_side_tables(ls, r == 0 ? 4 : 3, side, c->tables.side_off[ls][r]);
         if ((e = cudaMalloc(&c->tables.side, side.size() * sizeof(Tw))) != cudaSuccess ||
             (e = cudaMemcpy(c->tables.side, side.data(), side.size() * sizeof(Tw), cudaMemcpyHostToDevice)) !=
                 cudaSuccess) {

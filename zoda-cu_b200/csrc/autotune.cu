@@ -9,9 +9,9 @@
 // fastest survivor becomes the side's plan on the context.
 //
 // Candidates: the direct-load kernel with either radix schedule and either
-// tile order; the TMA-staged kernel (sides >= 32) with L2 promotion 256 B,
-// 128 B or none, either tile order, and the warp-group stagger at each of its
-// three release points or off.
+// tile order; the TMA-staged kernel (sides >= 32) with radix-16 or radix-8
+// levels (512 or 1024 threads), L2 promotion 256 B or none, either tile order,
+// and the warp-group stagger released late, early or off.
 #include <algorithm>
 #include <vector>
 
@@ -54,7 +54,7 @@ std::vector<zoda_plan> candidates(int ls) {
     c.push_back(d);
     auto same = [](const zoda_plan& a, const zoda_plan& b) {
         return a.impl == b.impl && a.sched == b.sched && a.l2_promo == b.l2_promo && a.blocked == b.blocked &&
-               a.stagger == b.stagger;
+               a.stagger == b.stagger && a.radix == b.radix;
     };
     auto add = [&](zoda_plan p) {
         for (const auto& q : c)
@@ -69,19 +69,22 @@ std::vector<zoda_plan> candidates(int ls) {
             p.blocked = blocked;
             p.l2_promo = 3;
             p.stagger = 1;
+            p.radix = 16;
             add(p);
         }
         if (ls >= 5)
-            for (int promo : {3, 2, 0})
-                for (int stagger : {1, 2, 3, 0}) {
-                    zoda_plan p = d;
-                    p.impl = ZODA_IMPL_TMA;
-                    p.sched = 0;
-                    p.l2_promo = promo;
-                    p.blocked = blocked;
-                    p.stagger = stagger;
-                    add(p);
-                }
+            for (int radix : {16, 8})
+                for (int promo : {3, 0})
+                    for (int stagger : {1, 2, 0}) {
+                        zoda_plan p = d;
+                        p.impl = ZODA_IMPL_TMA;
+                        p.sched = 0;
+                        p.l2_promo = promo;
+                        p.blocked = blocked;
+                        p.stagger = stagger;
+                        p.radix = radix;
+                        add(p);
+                    }
     }
     return c;
 }

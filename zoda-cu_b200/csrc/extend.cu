@@ -29,19 +29,19 @@ zoda_status launch_t(const zoda_ctx* ctx, const uint32_t* in, uint32_t* out, uin
     return ZODA_OK;
 }
 
-template <int LOG_S>
+template <int LOG_S, int LEPT>
 zoda_status launch_tma_t(const zoda_ctx* ctx, const uint32_t* in, uint32_t* out, uint64_t cols, int promo,
                          uint32_t flags, cudaStream_t st) {
-    using TP = TPlan<LOG_S>;
+    using TP = TPlan<LOG_S, LEPT>;
     const uint64_t ntiles = (cols + TP::C - 1) / TP::C;
     if (ntiles == 0) return ZODA_OK;
     CUtensorMap m_in, m_even;
     zoda_status s = make_tile_maps<TP>(&m_in, &m_even, in, out, cols, promo);
     if (s != ZODA_OK) return s;
     const uint64_t grid = ntiles < (uint64_t)ctx->sm_count ? ntiles : (uint64_t)ctx->sm_count;
-    const SideTables tb = side_tables(ctx, LOG_S);
-    k_extend_tma<LOG_S><<<(unsigned)grid, 512, TP::SMEM, st>>>(m_in, m_even, out, cols, ntiles, tb, ctx->d_err,
-                                                               flags);
+    const SideTables tb = side_tables(ctx, LOG_S, LEPT);
+    k_extend_tma<LOG_S, LEPT><<<(unsigned)grid, TP::THREADS, TP::SMEM, st>>>(m_in, m_even, out, cols, ntiles, tb,
+                                                                            ctx->d_err, flags);
     ZB_CUDA(cudaGetLastError());
     return ZODA_OK;
 }
@@ -59,9 +59,12 @@ zoda_status set_attr_t() {
             ZB_CUDA(cudaFuncSetAttribute(k_extend<LOG_S, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)ExtPlan<LOG_S, 1>::SMEM));
     }
-    if constexpr (LOG_S >= 5)
-        ZB_CUDA(cudaFuncSetAttribute(k_extend_tma<LOG_S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)TPlan<LOG_S>::SMEM));
+    if constexpr (LOG_S >= 5) {
+        ZB_CUDA(cudaFuncSetAttribute(k_extend_tma<LOG_S, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)TPlan<LOG_S, 4>::SMEM));
+        ZB_CUDA(cudaFuncSetAttribute(k_extend_tma<LOG_S, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)TPlan<LOG_S, 3>::SMEM));
+    }
     return ZODA_OK;
 }
 
@@ -94,6 +97,7 @@ zoda_plan default_plan(int log_s) {
     p.l2_promo = 3;
     p.blocked = 0;
     p.stagger = 1;
+    p.radix = 16;
     p.ms = 0.f;
     return p;
 }
@@ -103,8 +107,9 @@ zoda_status check_plan(int log_s, const zoda_plan& p) {
     if (p.impl != ZODA_IMPL_DIRECT && p.impl != ZODA_IMPL_TMA) return ZODA_ERR_ARG;
     if (p.impl == ZODA_IMPL_TMA && log_s < 5) return ZODA_ERR_UNSUPPORTED;
     if (p.sched < 0 || p.sched > 1 || p.l2_promo < 0 || p.l2_promo > 3 || p.blocked < 0 || p.blocked > 1 ||
-        p.stagger < 0 || p.stagger > 3)
+        p.stagger < 0 || p.stagger > 3 || (p.radix != 16 && p.radix != 8))
         return ZODA_ERR_ARG;
+    if (p.radix == 8 && p.impl != ZODA_IMPL_TMA) return ZODA_ERR_UNSUPPORTED;
     return ZODA_OK;
 }
 
@@ -123,8 +128,10 @@ zoda_status launch_plan(const zoda_ctx* ctx, int log_s, const zoda_plan& p, cons
     const uint32_t flags = (p.blocked ? 1u : 0u) | (p.stagger ? 0u : 2u) | (at_code << 2);
     if (p.impl == ZODA_IMPL_TMA) {
         switch (log_s) {
-#define ZB_CASE(L) \
-    case L: return launch_tma_t<L>(ctx, in, out, cols, p.l2_promo, flags, st);
+#define ZB_CASE(L)                                                                  \
+    case L:                                                                         \
+        return p.radix == 8 ? launch_tma_t<L, 3>(ctx, in, out, cols, p.l2_promo, flags, st) \
+                            : launch_tma_t<L, 4>(ctx, in, out, cols, p.l2_promo, flags, st);
             ZB_CASE(5) ZB_CASE(6) ZB_CASE(7) ZB_CASE(8) ZB_CASE(9) ZB_CASE(10) ZB_CASE(11) ZB_CASE(12)
 #undef ZB_CASE
             default: return ZODA_ERR_UNSUPPORTED;

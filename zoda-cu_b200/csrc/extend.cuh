@@ -29,22 +29,26 @@ constexpr int TW_N = 1 << LOG_TW;
 // SCHED picks where the leftover radix goes when LOG_S is not a multiple of 4:
 // 0 = the INTT's last level (and the NTT's first), 1 = the INTT's first level
 // (and the NTT's last). The autotuner chooses per side.
-template <int LOG_S_, int SCHED_ = 0>
+// LEPT_ is the log2 of the level radix and of the positions a thread holds
+// per column (4: radix 16; 3: radix 8 with half the registers, so twice the
+// threads fit), THREADS_ the CTA size.
+template <int LOG_S_, int SCHED_ = 0, int LEPT_ = 4, int THREADS_ = 512>
 struct ExtPlan {
     static constexpr int LOG_S = LOG_S_;
     static constexpr int SCHED = SCHED_;
+    static constexpr int LEPT = LEPT_;
     static constexpr int S = 1 << LOG_S;
-    static constexpr int NLEV = (LOG_S + 3) / 4;  // INTT levels (= NTT levels)
-    static constexpr int EPT = LOG_S >= 4 ? 16 : S;
+    static constexpr int NLEV = (LOG_S + LEPT - 1) / LEPT;  // INTT levels (= NTT levels)
+    static constexpr int EPT = LOG_S >= LEPT ? 1 << LEPT : S;
     static constexpr int TPQ = S / EPT;  // threads per column quad
-    static constexpr int THREADS = 512;
+    static constexpr int THREADS = THREADS_;
     static constexpr int Q4 = THREADS / TPQ;  // column quads per tile
     static constexpr int C = 4 * Q4;          // columns per tile
     static constexpr size_t SMEM = NLEV > 1 ? (size_t)S * Q4 * 16 : 0;
-    static constexpr int LEFT = LOG_S - 4 * (NLEV - 1);  // the leftover level's log2 radix
+    static constexpr int LEFT = LOG_S - LEPT * (NLEV - 1);  // the leftover level's log2 radix
     // log2 radix of INTT level l; the NTT runs them in reverse order
     __host__ __device__ static constexpr int lr(int l) {
-        return SCHED == 0 ? (l < NLEV - 1 ? 4 : LEFT) : (l == 0 ? LEFT : 4);
+        return SCHED == 0 ? (l < NLEV - 1 ? LEPT : LEFT) : (l == 0 ? LEFT : LEPT);
     }
     __host__ __device__ static constexpr int nlr(int l) { return lr(NLEV - 1 - l); }
     __host__ __device__ static constexpr int pre(int l) {

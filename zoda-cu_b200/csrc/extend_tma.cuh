@@ -67,17 +67,19 @@ __device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, int x, int 
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-__device__ __forceinline__ void group_bar(int id) { asm volatile("bar.sync %0, 256;" ::"r"(id) : "memory"); }
+__device__ __forceinline__ void group_bar(int id, int count = 256) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
-// OR of a predicate over one warp-group, through its named barrier.
-__device__ __forceinline__ bool group_vote_or(int id, bool v) {
+// OR of a predicate over one warp-group of `count` threads, through its named barrier.
+__device__ __forceinline__ bool group_vote_or(int id, bool v, int count = 256) {
     uint32_t r;
     asm volatile(
-        "{\n .reg .pred p, q;\n setp.ne.u32 q, %2, 0;\n bar.red.or.pred p, %1, 256, q;\n selp.u32 %0, 1, 0, p;\n}"
+        "{\n .reg .pred p, q;\n setp.ne.u32 q, %2, 0;\n bar.red.or.pred p, %1, %3, q;\n selp.u32 %0, 1, 0, p;\n}"
         : "=r"(r)
-        : "r"(id), "r"((uint32_t)v)
+        : "r"(id), "r"((uint32_t)v), "r"(count)
         : "memory");
     return r != 0;
 }
@@ -91,24 +93,45 @@ __device__ __forceinline__ bool group_vote_or(int id, bool v) {
 //   * exchange: word(slot, q) = slot*GQ + q + sum PW*(slot >> PS), a padding that
 //     stays additive in the register index, so addresses keep immediate offsets;
 //   * twiddle tables live in HBM/L1 in [k2][index] order (see SideTables).
-// staging-conflict-free lane map for side 1024 (basis images of the 3 low bits)
-constexpr int PERM10_B0 = 5, PERM10_B1 = 2, PERM10_B2 = 1;
-
+// Exchange padding word(slot) += PW1*(slot >> PS1) + PW2*(slot >> PS2) and
+// the lane map's basis images PB0..PB2, per side and level radix, found with a
+// bank model of every staging read and exchange access (conflict free except
+// a 2-way case in one radix-16 exchange at side 512 and a few radix-8 ones at
+// side 4096).
+template <int LOG_S, int LEPT>
+struct XPad;
 template <int LOG_S>
-struct XPad {  // exchange padding word(slot) += PW1*(slot >> PS1) + PW2*(slot >> PS2), per side
+struct XPad<LOG_S, 4> {
     static constexpr int PS1 = LOG_S == 9 ? 1 : LOG_S == 10 ? 3 : LOG_S == 11 ? 3 : LOG_S == 12 ? 4 : 0;
     static constexpr int PW1 = LOG_S == 9 ? 1 : LOG_S == 10 ? 8 : LOG_S == 11 ? 2 : LOG_S == 12 ? 1 : 0;
     static constexpr int PS2 = LOG_S == 10 ? 4 : LOG_S == 11 ? 6 : 0;
     static constexpr int PW2 = LOG_S == 10 ? 4 : LOG_S == 11 ? 2 : 0;
+    static constexpr int PB0 = LOG_S == 10 ? 5 : 1;
+    static constexpr int PB1 = LOG_S == 10 ? 2 : LOG_S == 11 ? 4 : 2;
+    static constexpr int PB2 = LOG_S == 10 ? 1 : LOG_S == 11 ? 2 : 4;
+};
+template <int LOG_S>
+struct XPad<LOG_S, 3> {  // radix 8, 1024 threads (side 4096 keeps a few 2-way conflicts)
+    static constexpr int PS1 = LOG_S == 9 ? 1 : LOG_S == 10 ? 3 : LOG_S == 11 ? 3 : LOG_S == 12 ? 4 : 0;
+    static constexpr int PW1 = LOG_S == 9 ? 1 : LOG_S == 10 ? 4 : LOG_S == 11 ? 2 : LOG_S == 12 ? 2 : 0;
+    static constexpr int PS2 = LOG_S == 9 ? 2 : LOG_S == 10 ? 6 : LOG_S == 11 ? 6 : LOG_S == 12 ? 7 : 0;
+    static constexpr int PW2 = LOG_S == 9 ? 2 : LOG_S == 10 ? 4 : LOG_S == 11 ? 2 : LOG_S == 12 ? 1 : 0;
+    static constexpr int PB0 = LOG_S == 10 ? 5 : 1;
+    static constexpr int PB1 = LOG_S == 10 ? 3 : LOG_S == 11 ? 4 : 2;
+    static constexpr int PB2 = LOG_S == 10 ? 1 : LOG_S == 11 ? 2 : 4;
 };
 
-template <int LOG_S_>
+// LEPT_ 4: radix-16 levels, 512 threads; 3: radix-8 levels, 1024 threads.
+template <int LOG_S_, int LEPT_ = 4>
 struct TPlan {
-    using PL = ExtPlan<LOG_S_>;  // whole-CTA view: 512 threads, Q4 quads, C columns
+    using PL = ExtPlan<LOG_S_, 0, LEPT_, LEPT_ == 3 ? 1024 : 512>;  // whole-CTA view: Q4 quads, C columns
     static constexpr int LOG_S = LOG_S_;
+    static constexpr int LEPT = LEPT_;
     static constexpr int S = PL::S, C = PL::C, Q4 = PL::Q4, TPQ = PL::TPQ, EPT = PL::EPT;
     static constexpr int NLEV = PL::NLEV;
-    static constexpr int GQ = Q4 / 2;  // quads per warp-group
+    static constexpr int THREADS = PL::THREADS;
+    static constexpr int GS = THREADS / 2;  // threads per warp-group
+    static constexpr int GQ = Q4 / 2;       // quads per warp-group
     // TMA boxes: at most 256 rows x 256 columns; sides below 128 have tiles wider
     // than 256 columns and stage them as NBOXC column boxes side by side.
     static constexpr int BOX_R = S < 256 ? S : 256;
@@ -120,14 +143,12 @@ struct TPlan {
     static constexpr int ROW_BYTES = BOX_C * 4;
     static constexpr uint32_t SWZ_MASK = ROW_BYTES == 128 ? 7 : ROW_BYTES == 64 ? 3 : ROW_BYTES == 32 ? 1 : 0;
     static constexpr int QB = BOX_C / 4;  // quads per box row
-    using XP = XPad<LOG_S>;
+    using XP = XPad<LOG_S, LEPT_>;
     // Lane map inside a warp: quad ql = lane % GQ, row group t = TW*warp + perm(lane / GQ),
     // perm a bit-linear map (images of the basis vectors) chosen, together with the
     // exchange padding, so staging reads and every exchange access are conflict free.
     static constexpr int TW = GQ < 32 ? 32 / GQ : 1;
-    static constexpr int PB0 = LOG_S == 11 ? 1 : LOG_S == 10 ? PERM10_B0 : 1;
-    static constexpr int PB1 = LOG_S == 11 ? 4 : LOG_S == 10 ? PERM10_B1 : 2;
-    static constexpr int PB2 = LOG_S == 11 ? 2 : LOG_S == 10 ? PERM10_B2 : 4;
+    static constexpr int PB0 = XP::PB0, PB1 = XP::PB1, PB2 = XP::PB2;
     __device__ static __forceinline__ int lane_t(int x) {  // x = lane / GQ in [0, TW)
         int y = x & ~7;
         if (x & 1) y ^= PB0;
@@ -142,6 +163,7 @@ struct TPlan {
     static constexpr size_t OFF_BAR = (OFF_X + 2 * X_BYTES + 15) / 16 * 16;
     static constexpr size_t SMEM = OFF_BAR + 32;
     static_assert(LOG_S >= 5 && LOG_S <= 12, "TMA path covers sides 32..4096");
+    static_assert(NLEV <= 4, "level tables cover four levels");
     static_assert(GQ >= 1, "two warp-groups");
     static_assert(NLEV >= 2, "at least one exchange");
     static_assert(SMEM <= 232448, "shared memory budget");
@@ -177,9 +199,9 @@ struct TPlan {
 // where level geometry (N, L, R) is that of ExtPlan, b the INTT last-level
 // block, c0(b) its first coefficient index.
 struct SideTables {
-    const uint2* intt[2];
+    const uint2* intt[3];
     const uint2* ntt0;
-    const uint2* ntt[2];
+    const uint2* ntt[3];
 };
 
 // Twiddle functors: get<K>() returns the factor for output k2 = K.
@@ -272,14 +294,14 @@ __device__ __forceinline__ void exchange(V4* v, uint2* xg, int ql, int bar, cons
     for (int g = 0; g < GR; g++) rb[g] = TP::xword(rbase(g), ql);
 #pragma unroll
     for (int h = 0; h < 2; h++) {
-        group_bar(bar);
+        group_bar(bar, TP::GS);
 #pragma unroll
         for (int g = 0; g < GW; g++)
 #pragma unroll
             for (int r = 0; r < RW; r++)
                 xg[wb[g] + TP::xoff((uint32_t)bitrev(r, LRW) << WSH)] =
                     make_uint2(v[g * RW + r].c[2 * h], v[g * RW + r].c[2 * h + 1]);
-        group_bar(bar);
+        group_bar(bar, TP::GS);
 #pragma unroll
         for (int g = 0; g < GR; g++)
 #pragma unroll
@@ -295,9 +317,10 @@ __device__ __forceinline__ void exchange(V4* v, uint2* xg, int ql, int bar, cons
 // run by the kernel body.
 // With stagger_pending set, group 0 releases group 1 (named barrier 3) as it
 // starts INTT level `stagger_at`.
+template <int THREADS>
 __device__ __forceinline__ void stagger_release(bool& stagger_pending) {
     if (stagger_pending) {
-        asm volatile("bar.arrive 3, 512;" ::: "memory");
+        asm volatile("bar.arrive 3, %0;" ::"n"(THREADS) : "memory");
         stagger_pending = false;
     }
 }
@@ -305,7 +328,7 @@ template <class TP, int l>
 __device__ __forceinline__ void intt_upto_last(V4* v, uint2* xg, int t, int ql, int bar, const SideTables& tb,
                                                bool& stagger_pending, int stagger_at) {
     if constexpr (l < TP::NLEV - 1) {
-        if (l == stagger_at) stagger_release(stagger_pending);
+        if (l == stagger_at) stagger_release<TP::THREADS>(stagger_pending);
         using W = LvlGeom<TP, TP::lr(l), TP::pre(l)>;
         using Rd = LvlGeom<TP, TP::lr(l + 1), TP::pre(l + 1)>;
 #pragma unroll
@@ -405,7 +428,7 @@ __device__ __forceinline__ void tile_compute(V4* v, uint2* xg, const Coords<TP>&
     const int t = c.t, ql = c.ql;
     // ---- INTT levels 0 .. NLEV-2
     intt_upto_last<TP, 0>(v, xg, t, ql, bar, tb, stagger_pending, stagger_at);
-    stagger_release(stagger_pending);
+    stagger_release<TP::THREADS>(stagger_pending);
     {
         // ---- INTT last level (L = 1). Its outputs need the twist g^c / S with
         // c = c0 + k2*S/R; g^(k2*S/R) = omega_2R^k2 is an immediate folded into the
@@ -450,22 +473,22 @@ __device__ __forceinline__ int opaque(int x) {
 // flags: bit 0 = blocked tile order (TileRange), bit 1 = no stagger between the
 // warp-groups, bits 2-3 = the INTT level at which group 0 releases group 1,
 // plus one (0: the default, after all INTT levels but the last).
-template <int LOG_S>
-__global__ void __launch_bounds__(512, 1)
+template <int LOG_S, int LEPT = 4>
+__global__ void __launch_bounds__(TPlan<LOG_S, LEPT>::THREADS, 1)
     k_extend_tma(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_even,
                  uint32_t* __restrict__ out, uint64_t cols, uint64_t ntiles, const SideTables tb,
                  int* __restrict__ err, uint32_t flags) {
-    using TP = TPlan<LOG_S>;
+    using TP = TPlan<LOG_S, LEPT>;
     extern __shared__ __align__(1024) unsigned char smem[];
     uint32_t* stage = reinterpret_cast<uint32_t*>(smem);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + TP::OFF_BAR);   // tile landed (TMA tx)
     uint64_t* empty = full + 1;                                          // both groups copied it out
     const int tid = threadIdx.x;
-    const int grp = tid >> 8;
+    const int grp = tid / TP::GS;
     const int bar = 1 + grp;
-    // Thread 256 (first thread of group 1, the group that reads the staging
-    // buffer last) is the producer: it issues every TMA load and even-row store.
-    const bool producer = tid == 256;
+    // The first thread of group 1 (the group that reads the staging buffer
+    // last) is the producer: it issues every TMA load and even-row store.
+    const bool producer = tid == TP::GS;
     if (tid == 0) {
         mbar_init(full, 1);
         mbar_init(empty, 2);
@@ -479,18 +502,18 @@ __global__ void __launch_bounds__(512, 1)
     if (producer && tile < tr.last) tma_load_tile<TP>(stage, &tm_in, tile, full);
     // Group 1 starts half a tile after group 0 so the two groups' barriers and
     // butterfly phases interleave; group 0 signals from the middle of its first tile.
-    if (stagger && grp == 1 && tile < tr.last) asm volatile("bar.sync 3, 512;" ::: "memory");
+    if (stagger && grp == 1 && tile < tr.last) asm volatile("bar.sync 3, %0;" ::"n"(TP::THREADS) : "memory");
     bool stagger_pending = stagger && grp == 0 && tile < tr.last;
     V4 v[TP::EPT];
     uint32_t parity = 0;
     for (; tile < tr.last; tile += tr.step, parity ^= 1) {
         const int tid_l = opaque(tid);
-        const Coords<TP> c(tid_l & 255, grp);
-        uint2* xg = reinterpret_cast<uint2*>(smem + TP::OFF_X + (tid_l >> 8) * TP::X_BYTES);
+        const Coords<TP> c(tid_l % TP::GS, grp);
+        uint2* xg = reinterpret_cast<uint2*>(smem + TP::OFF_X + (tid_l / TP::GS) * TP::X_BYTES);
         const bool ok = mbar_wait_bounded(full, parity);
-        if (group_vote_or(bar, !ok)) {
-            if ((tid & 255) == 0) atomicOr(err, 1);
-            if (stagger_pending) asm volatile("bar.arrive 3, 512;" ::: "memory");
+        if (group_vote_or(bar, !ok, TP::GS)) {
+            if (tid % TP::GS == 0) atomicOr(err, 1);
+            stagger_release<TP::THREADS>(stagger_pending);
             if (producer) bulk_wait0();
             return;
         }
@@ -498,8 +521,8 @@ __global__ void __launch_bounds__(512, 1)
         const uint64_t col = tile * TP::C + 4 * (uint64_t)c.q;
         const bool active = col < cols;
         stage_read<TP>(v, smem, c);
-        group_bar(bar);  // this group has copied the staging buffer out
-        if ((tid & 255) == 0) mbar_arrive(empty);
+        group_bar(bar, TP::GS);  // this group has copied the staging buffer out
+        if (tid % TP::GS == 0) mbar_arrive(empty);
         const uint64_t next = tile + tr.step;
         if (producer && next < tr.last) {
             const bool e_ok = mbar_wait_bounded(empty, parity);  // the other group is done too
@@ -510,7 +533,7 @@ __global__ void __launch_bounds__(512, 1)
         }
         tile_compute<TP>(v, xg, c, bar, tb, out, cols, col, active, stagger_pending, stagger_at);
     }
-    if (stagger_pending) asm volatile("bar.arrive 3, 512;" ::: "memory");
+    stagger_release<TP::THREADS>(stagger_pending);
     if (producer) bulk_wait0();
 }
 

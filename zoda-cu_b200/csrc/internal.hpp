@@ -41,7 +41,8 @@ struct Tables {
     Tw* twist = nullptr;
     // per-side level tables of the TMA-staged kernels (log2 side 5..12), one buffer
     Tw* side = nullptr;
-    size_t side_off[13][5] = {};  // [log_s][intt0, intt1, ntt0, ntt1, end] entry offsets
+    // [log_s][radix 16, radix 8][intt0, intt1, intt2, ntt0, ntt1, ntt2, end] entry offsets
+    size_t side_off[13][2][8] = {};
 };
 
 }  // namespace zb

@@ -61,16 +61,17 @@ zoda_status make_tile_maps(CUtensorMap* m_in, CUtensorMap* m_even, const uint32_
     return make_map(m_even, out, cols, TP::S, cols * 8, TP::BOX_C, TP::BOX_R, swz);
 }
 
-// Device pointers of the side's level tables (built in zoda_ctx_create).
-inline SideTables side_tables(const zoda_ctx* ctx, int log_s) {
+// Device pointers of the side's level tables (built in zoda_ctx_create) for
+// level radix 2^lept (4 or 3).
+inline SideTables side_tables(const zoda_ctx* ctx, int log_s, int lept = 4) {
     SideTables tb;
-    const size_t* off = ctx->tables.side_off[log_s];
+    const size_t* off = ctx->tables.side_off[log_s][lept == 3 ? 1 : 0];
     const uint2* base = reinterpret_cast<const uint2*>(ctx->tables.side);
-    tb.intt[0] = base + off[0];
-    tb.intt[1] = base + off[1];
-    tb.ntt0 = base + off[2];
+    for (int l = 0; l < 3; l++) tb.intt[l] = base + off[l];
+    tb.ntt0 = base + off[3];
     tb.ntt[0] = nullptr;  // NTT level 0 reads ntt0
-    tb.ntt[1] = base + off[3];
+    tb.ntt[1] = base + off[4];
+    tb.ntt[2] = base + off[5];
     return tb;
 }
 

@@ -80,15 +80,17 @@ class ZodaTiming(ctypes.Structure):
 class ZodaPlan(ctypes.Structure):
     """Per-side launch plan (include/zoda_b200.h, zoda_plan)."""
     _fields_ = [("impl", ctypes.c_int32), ("sched", ctypes.c_int32), ("l2_promo", ctypes.c_int32),
-                ("blocked", ctypes.c_int32), ("stagger", ctypes.c_int32), ("ms", ctypes.c_float)]
-    KEYS = ("impl", "sched", "l2_promo", "blocked", "stagger", "ms")
+                ("blocked", ctypes.c_int32), ("stagger", ctypes.c_int32), ("radix", ctypes.c_int32),
+                ("ms", ctypes.c_float)]
+    KEYS = ("impl", "sched", "l2_promo", "blocked", "stagger", "radix", "ms")
+    DEFAULTS = {"radix": 16}
 
     def to_dict(self) -> dict:
         return {k: (round(float(getattr(self, k)), 5) if k == "ms" else int(getattr(self, k))) for k in self.KEYS}
 
     @classmethod
     def from_dict(cls, d: dict) -> "ZodaPlan":
-        return cls(*[d.get(k, 0) for k in cls.KEYS])
+        return cls(*[d.get(k, cls.DEFAULTS.get(k, 0)) for k in cls.KEYS])
 
 
 def load(path: str = LIB_PATH):
