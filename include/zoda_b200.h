@@ -106,16 +106,17 @@ zoda_status zoda_ctx_set_impl(zoda_ctx* ctx, int impl);
  * differs. */
 typedef struct zoda_plan {
     int32_t impl;     /* ZODA_IMPL_DIRECT or ZODA_IMPL_TMA (k >= 32)                   */
-    int32_t sched;    /* direct kernel: radix-16 levels with the leftover radix at the
-                         INTT's last level (0) or its first level (1)                  */
+    int32_t sched;    /* direct kernel: the leftover radix at the INTT's last level (0)
+                         or its first level (1)                                        */
     int32_t l2_promo; /* TMA kernel: L2 promotion of tile loads, 0 none, 1 64 B,
                          2 128 B, 3 256 B                                              */
     int32_t blocked;  /* 0 = CTA i takes tiles i, i + grid, ...; 1 = one contiguous run */
     int32_t stagger;  /* TMA kernel: 0 = the two warp-groups run in step; 1, 2, 3 = the
                          second starts once the first begins its last INTT level, its
                          second INTT level, or its first (less apart, more shared code) */
-    int32_t radix;    /* TMA kernel: level radix 16 (512 threads, 16 positions per
-                         thread) or 8 (1024 threads, 8 positions: twice the warps) */
+    int32_t radix;    /* level radix 16 (512 threads, 16 positions per thread) or 8
+                         (1024 threads, 8 positions: twice the warps; direct kernel
+                         from k = 64)                                              */
     float ms;         /* the tuner's time for this plan (0 when set by hand)            */
 } zoda_plan;
 

@@ -50,6 +50,9 @@ def plans_for(side: int):
     for blocked in (0, 1):
         for sched in ((0, 1) if ls >= 5 and ls % 4 else (0,)):
             out.append(dict(impl=1, sched=sched, l2_promo=3, blocked=blocked, stagger=1))
+        if ls >= 6:
+            for sched in ((0, 1) if ls % 3 else (0,)):
+                out.append(dict(impl=1, sched=sched, l2_promo=3, blocked=blocked, stagger=1, radix=8))
         if ls >= 5:
             for radix in (16, 8):
                 for promo in (3, 2, 0):
@@ -117,7 +120,7 @@ def test_plan_errors(ctx):
     with pytest.raises(zoda_b200.ZodaError):
         ctx.plan_set(64, dict(impl=2, sched=0, l2_promo=3, blocked=0, stagger=1, radix=4))
     with pytest.raises(zoda_b200.ZodaError):
-        ctx.plan_set(64, dict(impl=1, sched=0, l2_promo=3, blocked=0, stagger=1, radix=8))  # radix 8: TMA only
+        ctx.plan_set(32, dict(impl=1, sched=0, l2_promo=3, blocked=0, stagger=1, radix=8))  # direct radix 8 from 64
     with pytest.raises(zoda_b200.ZodaError):
         ctx.autotune(64, 32)
     assert ctx.plan_get(1024) is None

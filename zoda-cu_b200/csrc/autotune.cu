@@ -8,8 +8,8 @@
 // back-to-back launches with CUDA events on the context's stream. The
 // fastest survivor becomes the side's plan on the context.
 //
-// Candidates: the direct-load kernel with either radix schedule and either
-// tile order; the TMA-staged kernel (sides >= 32) with radix-16 or radix-8
+// Candidates: the direct-load kernel with radix-16 or radix-8 levels (512 or
+// 1024 threads), either radix schedule and either tile order; the TMA-staged kernel (sides >= 32) with radix-16 or radix-8
 // levels (512 or 1024 threads), L2 promotion 256 B or none, either tile order,
 // and the warp-group stagger released late, early or off.
 #include <algorithm>
@@ -62,15 +62,19 @@ std::vector<zoda_plan> candidates(int ls) {
         c.push_back(p);
     };
     for (int blocked = 0; blocked <= 1; blocked++) {
-        for (int sched = 0; sched <= (distinct_sched1(ls) ? 1 : 0); sched++) {
-            zoda_plan p = d;
-            p.impl = ZODA_IMPL_DIRECT;
-            p.sched = sched;
-            p.blocked = blocked;
-            p.l2_promo = 3;
-            p.stagger = 1;
-            p.radix = 16;
-            add(p);
+        for (int radix : {16, 8}) {
+            if (radix == 8 && ls < 6) continue;
+            const bool s1 = radix == 16 ? distinct_sched1(ls) : ls % 3 != 0;
+            for (int sched = 0; sched <= (s1 ? 1 : 0); sched++) {
+                zoda_plan p = d;
+                p.impl = ZODA_IMPL_DIRECT;
+                p.sched = sched;
+                p.blocked = blocked;
+                p.l2_promo = 3;
+                p.stagger = 1;
+                p.radix = radix;
+                add(p);
+            }
         }
         if (ls >= 5)
             for (int radix : {16, 8})

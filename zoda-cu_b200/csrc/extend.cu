@@ -16,15 +16,16 @@ __global__ void k_extend_side1(const uint32_t* __restrict__ in, uint32_t* __rest
     }
 }
 
-template <int LOG_S, int SCHED>
+template <int LOG_S, int SCHED, int LEPT = 4>
 zoda_status launch_t(const zoda_ctx* ctx, const uint32_t* in, uint32_t* out, uint64_t cols, uint32_t flags,
                      cudaStream_t st) {
-    using PL = ExtPlan<LOG_S, SCHED>;
+    using PL = ExtPlan<LOG_S, SCHED, LEPT, LEPT == 3 ? 1024 : 512>;
     const uint64_t ntiles = (cols + PL::C - 1) / PL::C;
     if (ntiles == 0) return ZODA_OK;
     const uint64_t grid = ntiles < (uint64_t)ctx->sm_count ? ntiles : (uint64_t)ctx->sm_count;
-    k_extend<LOG_S, SCHED><<<(unsigned)grid, PL::THREADS, PL::SMEM, st>>>(in, out, cols, ntiles, ctx->tables.tw,
-                                                                          ctx->tables.twist, flags);
+    k_extend<LOG_S, SCHED, LEPT><<<(unsigned)grid, PL::THREADS, PL::SMEM, st>>>(in, out, cols, ntiles,
+                                                                                ctx->tables.tw, ctx->tables.twist,
+                                                                                flags);
     ZB_CUDA(cudaGetLastError());
     return ZODA_OK;
 }
@@ -47,8 +48,11 @@ zoda_status launch_tma_t(const zoda_ctx* ctx, const uint32_t* in, uint32_t* out,
 }
 
 // The leftover radix differs from 16 (so schedule 1 is a distinct kernel) for
-// these sides only.
+// these sides only; the same for radix 8.
 constexpr bool has_sched1(int ls) { return ls >= 5 && ls % 4 != 0; }
+constexpr bool has_sched1_r8(int ls) { return ls >= 6 && ls % 3 != 0; }
+// Sides with a radix-8 direct kernel.
+constexpr bool has_direct_r8(int ls) { return ls >= 6; }
 
 template <int LOG_S>
 zoda_status set_attr_t() {
@@ -58,6 +62,13 @@ zoda_status set_attr_t() {
         if constexpr (has_sched1(LOG_S))
             ZB_CUDA(cudaFuncSetAttribute(k_extend<LOG_S, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)ExtPlan<LOG_S, 1>::SMEM));
+    }
+    if constexpr (has_direct_r8(LOG_S)) {
+        ZB_CUDA(cudaFuncSetAttribute(k_extend<LOG_S, 0, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)ExtPlan<LOG_S, 0, 3, 1024>::SMEM));
+        if constexpr (has_sched1_r8(LOG_S))
+            ZB_CUDA(cudaFuncSetAttribute(k_extend<LOG_S, 1, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)ExtPlan<LOG_S, 1, 3, 1024>::SMEM));
     }
     if constexpr (LOG_S >= 5) {
         ZB_CUDA(cudaFuncSetAttribute(k_extend_tma<LOG_S, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -69,8 +80,15 @@ zoda_status set_attr_t() {
 }
 
 template <int LOG_S>
-zoda_status launch_direct(const zoda_ctx* ctx, int sched, const uint32_t* in, uint32_t* out, uint64_t cols,
-                          uint32_t flags, cudaStream_t st) {
+zoda_status launch_direct(const zoda_ctx* ctx, int sched, int radix, const uint32_t* in, uint32_t* out,
+                          uint64_t cols, uint32_t flags, cudaStream_t st) {
+    if constexpr (has_direct_r8(LOG_S)) {
+        if (radix == 8) {
+            if constexpr (has_sched1_r8(LOG_S))
+                if (sched == 1) return launch_t<LOG_S, 1, 3>(ctx, in, out, cols, flags, st);
+            return launch_t<LOG_S, 0, 3>(ctx, in, out, cols, flags, st);
+        }
+    }
     if constexpr (has_sched1(LOG_S))
         if (sched == 1) return launch_t<LOG_S, 1>(ctx, in, out, cols, flags, st);
     return launch_t<LOG_S, 0>(ctx, in, out, cols, flags, st);
@@ -109,7 +127,7 @@ zoda_status check_plan(int log_s, const zoda_plan& p) {
     if (p.sched < 0 || p.sched > 1 || p.l2_promo < 0 || p.l2_promo > 3 || p.blocked < 0 || p.blocked > 1 ||
         p.stagger < 0 || p.stagger > 3 || (p.radix != 16 && p.radix != 8))
         return ZODA_ERR_ARG;
-    if (p.radix == 8 && p.impl != ZODA_IMPL_TMA) return ZODA_ERR_UNSUPPORTED;
+    if (p.radix == 8 && p.impl == ZODA_IMPL_DIRECT && log_s < 6) return ZODA_ERR_UNSUPPORTED;
     return ZODA_OK;
 }
 
@@ -146,7 +164,7 @@ zoda_status launch_plan(const zoda_ctx* ctx, int log_s, const zoda_plan& p, cons
             return ZODA_OK;
         }
 #define ZB_CASE(L) \
-    case L: return launch_direct<L>(ctx, p.sched, in, out, cols, flags, st);
+    case L: return launch_direct<L>(ctx, p.sched, p.radix, in, out, cols, flags, st);
         ZB_CASE(1) ZB_CASE(2) ZB_CASE(3) ZB_CASE(4) ZB_CASE(5) ZB_CASE(6)
         ZB_CASE(7) ZB_CASE(8) ZB_CASE(9) ZB_CASE(10) ZB_CASE(11) ZB_CASE(12)
 #undef ZB_CASE

@@ -255,11 +255,12 @@ struct TileRange {
     }
 };
 
-template <int LOG_S, int SCHED = 0>
-__global__ void __launch_bounds__(512, 1)
+// LEPT 4: radix-16 levels, 512 threads; 3: radix-8 levels, 1024 threads.
+template <int LOG_S, int SCHED = 0, int LEPT = 4>
+__global__ void __launch_bounds__(LEPT == 3 ? 1024 : 512, 1)
     k_extend(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint64_t cols, uint64_t ntiles,
              const Tw* __restrict__ tw, const Tw* __restrict__ twist_all, uint32_t flags) {
-    using PL = ExtPlan<LOG_S, SCHED>;
+    using PL = ExtPlan<LOG_S, SCHED, LEPT, LEPT == 3 ? 1024 : 512>;
     extern __shared__ uint4 sm[];
     const int tid = threadIdx.x;
     const int q = tid % PL::Q4;
