@@ -143,3 +143,23 @@ def test_batch_follows_the_side_promotion(ctx):
             assert np.array_equal(o.cpu().numpy().view(np.uint32), O.encode_rowmajor(d))
     finally:
         ctx.plan_clear()
+
+
+@pytest.mark.parametrize("radix", [16, 8])
+def test_batch_runs_the_largest_sides_radix(ctx, radix):
+    import zoda_b200
+    sides = [32, 2048, 64, 512, 128, 1024, 256]
+    datas = [O.seeded_input(s, 3 * tile_cols(s) + 4, seed=90 + i) for i, s in enumerate(sides)]
+    ins = [to_dev(d) for d in datas]
+    outs = [torch.empty((2 * d.shape[0], d.shape[1]), dtype=torch.int32, device="cuda") for d in datas]
+    ctx.plan_set(2048, dict(impl=2, sched=0, l2_promo=3, blocked=0, stagger=1, radix=radix))
+    try:
+        b = zoda_b200.Batch(ctx, [(i, o, d.shape[0], d.shape[1]) for i, o, d in zip(ins, outs, datas)])
+        b.run()
+        torch.cuda.synchronize()
+        ctx.check()
+        b.close()
+        for d, o in zip(datas, outs):
+            assert np.array_equal(o.cpu().numpy().view(np.uint32), O.encode_rowmajor(d)), d.shape
+    finally:
+        ctx.plan_clear()

@@ -18,7 +18,8 @@ struct zoda_batch {
     uint64_t elements = 0;
     zb::DevBuf squares;  // BatchSquare[nsq]
     zb::DevBuf counter;  // unsigned long long
-    zb::DevBuf tables;   // SideTables[13]
+    zb::DevBuf tables;   // SideTables[26]: radix 16 at [log_s], radix 8 at [13 + log_s]
+    int lept = 4;        // level radix 2^lept of this batch's launch
     cudaStream_t cap = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -69,18 +70,32 @@ zoda_status make_batch_square(const zoda_square& q, BatchSquare* b, int promo) {
 }
 
 zoda_status launch_batch_kernel(const zoda_ctx* ctx, const BatchSquare* d_sq, uint32_t nsq, uint64_t total_tiles,
-                                unsigned long long* d_counter, const SideTables* d_tables, cudaStream_t st) {
+                                unsigned long long* d_counter, const SideTables* d_tables, int lept, cudaStream_t st) {
     if (total_tiles == 0) return ZODA_OK;
     const uint64_t grid = total_tiles < (uint64_t)ctx->sm_count ? total_tiles : (uint64_t)ctx->sm_count;
-    k_extend_batch<0><<<(unsigned)grid, 512, BATCH_SMEM, st>>>(d_sq, nsq, total_tiles, d_counter, d_tables,
-                                                                ctx->d_err);
+    if (lept == 3)
+        k_extend_batch<3><<<(unsigned)grid, BatchGeom<3>::THREADS, BatchGeom<3>::SMEM, st>>>(
+            d_sq, nsq, total_tiles, d_counter, d_tables, ctx->d_err);
+    else
+        k_extend_batch<4><<<(unsigned)grid, BatchGeom<4>::THREADS, BatchGeom<4>::SMEM, st>>>(
+            d_sq, nsq, total_tiles, d_counter, d_tables, ctx->d_err);
     ZB_CUDA(cudaGetLastError());
     return ZODA_OK;
 }
 
 zoda_status set_batch_kernel_attributes() {
-    ZB_CUDA(cudaFuncSetAttribute(k_extend_batch<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BATCH_SMEM));
+    ZB_CUDA(cudaFuncSetAttribute(k_extend_batch<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)BatchGeom<4>::SMEM));
+    ZB_CUDA(cudaFuncSetAttribute(k_extend_batch<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)BatchGeom<3>::SMEM));
     return ZODA_OK;
+}
+
+int batch_lept(const zoda_ctx* ctx, int max_log) {
+    if (max_log >= 0 && max_log <= 12 && ctx->planned[max_log] && ctx->plan[max_log].impl == ZODA_IMPL_TMA &&
+        ctx->plan[max_log].radix == 8)
+        return 3;
+    return 4;
 }
 
 }  // namespace zb
@@ -124,15 +139,19 @@ zoda_status zoda_batch_create(zoda_ctx* ctx, const zoda_square* squares, uint32_
     zoda_status s;
     if ((s = bt->squares.ensure(std::max<size_t>(1, n) * sizeof(BatchSquare))) != ZODA_OK) return fail(s);
     if ((s = bt->counter.ensure(sizeof(unsigned long long))) != ZODA_OK) return fail(s);
-    if ((s = bt->tables.ensure(13 * sizeof(SideTables))) != ZODA_OK) return fail(s);
-    std::vector<SideTables> tabs(13);
-    for (int ls = BATCH_MIN_LOG; ls <= BATCH_MAX_LOG; ls++) tabs[ls] = side_tables(ctx, ls);
+    if ((s = bt->tables.ensure(26 * sizeof(SideTables))) != ZODA_OK) return fail(s);
+    std::vector<SideTables> tabs(26);
+    for (int ls = BATCH_MIN_LOG; ls <= BATCH_MAX_LOG; ls++) {
+        tabs[ls] = side_tables(ctx, ls, 4);
+        tabs[13 + ls] = side_tables(ctx, ls, 3);
+    }
+    bt->lept = batch_lept(ctx, n ? log2_side(squares[order[0]].k) : 0);
     if (n && (e = cudaMemcpy(bt->squares.p, host.data(), n * sizeof(BatchSquare), cudaMemcpyHostToDevice)) !=
                  cudaSuccess) {
         set_last_error("cudaMemcpy(batch squares)", e);
         return fail(ZODA_ERR_CUDA);
     }
-    if ((e = cudaMemcpy(bt->tables.p, tabs.data(), 13 * sizeof(SideTables), cudaMemcpyHostToDevice)) != cudaSuccess) {
+    if ((e = cudaMemcpy(bt->tables.p, tabs.data(), 26 * sizeof(SideTables), cudaMemcpyHostToDevice)) != cudaSuccess) {
         set_last_error("cudaMemcpy(batch tables)", e);
         return fail(ZODA_ERR_CUDA);
     }
@@ -151,9 +170,9 @@ zoda_status zoda_batch_run(zoda_batch* bt, void* stream) {
         ZB_CUDA(cudaStreamCreateWithFlags(&bt->cap, cudaStreamNonBlocking));
         ZB_CUDA(cudaStreamBeginCapture(bt->cap, cudaStreamCaptureModeThreadLocal));
         cudaMemsetAsync(bt->counter.p, 0, sizeof(unsigned long long), bt->cap);
-        const zoda_status ls = launch_batch_kernel(ctx, (const BatchSquare*)bt->squares.p, bt->nsq, bt->total_tiles,
-                                                   (unsigned long long*)bt->counter.p,
-                                                   (const SideTables*)bt->tables.p, bt->cap);
+        const zoda_status ls = launch_batch_kernel(
+            ctx, (const BatchSquare*)bt->squares.p, bt->nsq, bt->total_tiles, (unsigned long long*)bt->counter.p,
+            (const SideTables*)bt->tables.p + (bt->lept == 3 ? 13 : 0), bt->lept, bt->cap);
         cudaError_t e = cudaStreamEndCapture(bt->cap, &bt->graph);
         if (ls != ZODA_OK) return ls;
         if (e != cudaSuccess) {

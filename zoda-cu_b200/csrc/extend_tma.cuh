@@ -556,19 +556,25 @@ static_assert(sizeof(BatchSquare) % 64 == 0, "tensor maps stay 64-byte aligned")
 
 constexpr int BATCH_MIN_LOG = 5, BATCH_MAX_LOG = 11;
 constexpr size_t cmax(size_t a, size_t b) { return a > b ? a : b; }
-template <int L, int H>
+template <int L, int H, int LEPT>
 struct BatchLayout {
-    static constexpr size_t X = cmax(TPlan<L>::X_BYTES, BatchLayout<L + 1, H>::X);
+    static constexpr size_t X = cmax(TPlan<L, LEPT>::X_BYTES, BatchLayout<L + 1, H, LEPT>::X);
 };
-template <int H>
-struct BatchLayout<H, H> {
-    static constexpr size_t X = TPlan<H>::X_BYTES;
+template <int H, int LEPT>
+struct BatchLayout<H, H, LEPT> {
+    static constexpr size_t X = TPlan<H, LEPT>::X_BYTES;
 };
-constexpr size_t BATCH_X_BYTES = BatchLayout<BATCH_MIN_LOG, BATCH_MAX_LOG>::X;
-constexpr size_t BATCH_OFF_X = 128 * 1024;
-constexpr size_t BATCH_OFF_BAR = (BATCH_OFF_X + 2 * BATCH_X_BYTES + 15) / 16 * 16;
-constexpr size_t BATCH_SMEM = BATCH_OFF_BAR + 64;
-static_assert(BATCH_SMEM <= 232448, "shared memory budget");
+// Shared-memory layout of the batched kernel with level radix 2^LEPT:
+// 128 KB staging, the two groups' exchange buffers, barriers and the slot.
+template <int LEPT>
+struct BatchGeom {
+    static constexpr int THREADS = LEPT == 3 ? 1024 : 512;
+    static constexpr size_t X_BYTES = BatchLayout<BATCH_MIN_LOG, BATCH_MAX_LOG, LEPT>::X;
+    static constexpr size_t OFF_X = 128 * 1024;
+    static constexpr size_t OFF_BAR = (OFF_X + 2 * X_BYTES + 15) / 16 * 16;
+    static constexpr size_t SMEM = OFF_BAR + 64;
+    static_assert(SMEM <= 232448, "shared memory budget");
+};
 
 struct BatchSlot {  // descriptor of the tile in staging, written by the producer
     uint32_t sq;     // square index, or BATCH_END when the queue is drained
@@ -588,24 +594,25 @@ constexpr uint32_t BATCH_END = 0xFFFFFFFFu;
         default: CALL(11); break; \
     }
 
-// sq[0..nsq) sorted by first; total_tiles = sum of ntiles; *counter = 0 at launch.
-// (A template only so that the translation units that include this header but
-// never launch it do not compile it.)
-template <int UNUSED = 0>
-__global__ void __launch_bounds__(512, 1)
+// sq[0..nsq) sorted by first; total_tiles = sum of ntiles; *counter = 0 at
+// launch; tables[log_s] holds the level tables of radix 2^LEPT.
+template <int LEPT = 4>
+__global__ void __launch_bounds__(BatchGeom<LEPT>::THREADS, 1)
     k_extend_batch(const BatchSquare* __restrict__ sq, uint32_t nsq, uint64_t total_tiles,
                    unsigned long long* __restrict__ counter, const SideTables* __restrict__ tables,
                    int* __restrict__ err) {
+    using BG = BatchGeom<LEPT>;
+    constexpr int GS = BG::THREADS / 2;
     extern __shared__ __align__(1024) unsigned char smem[];
     uint32_t* stage = reinterpret_cast<uint32_t*>(smem);
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + BATCH_OFF_BAR);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + BG::OFF_BAR);
     uint64_t* empty = full + 1;
-    BatchSlot* slot = reinterpret_cast<BatchSlot*>(smem + BATCH_OFF_BAR + 16);
-    uint32_t* sq_hint = reinterpret_cast<uint32_t*>(smem + BATCH_OFF_BAR + 32);
+    BatchSlot* slot = reinterpret_cast<BatchSlot*>(smem + BG::OFF_BAR + 16);
+    uint32_t* sq_hint = reinterpret_cast<uint32_t*>(smem + BG::OFF_BAR + 32);
     const int tid = threadIdx.x;
-    const int grp = tid >> 8;
+    const int grp = tid / GS;
     const int bar = 1 + grp;
-    const bool producer = tid == 256;
+    const bool producer = tid == GS;
     if (tid == 0) {
         mbar_init(full, 1);
         mbar_init(empty, 2);
@@ -631,28 +638,28 @@ __global__ void __launch_bounds__(512, 1)
             mbar_arrive(full);  // completes the phase with no bytes: consumers see the end mark
         } else {
             const BatchSquare& b = sq[s.sq];
-#define ZB_LOAD(L) tma_load_tile<TPlan<L>>(stage, &b.in_map, s.tile, full)
+#define ZB_LOAD(L) tma_load_tile<TPlan<L, LEPT>>(stage, &b.in_map, s.tile, full)
             ZB_BATCH_SWITCH(s.log_s, ZB_LOAD)
 #undef ZB_LOAD
         }
     };
     if (producer) fetch();
-    if (grp == 1) asm volatile("bar.sync 3, 512;" ::: "memory");
+    if (grp == 1) asm volatile("bar.sync 3, %0;" ::"n"(BG::THREADS) : "memory");
     bool stagger_pending = grp == 0;
-    V4 v[16];
+    V4 v[1 << LEPT];
     uint32_t parity = 0;
     for (;; parity ^= 1) {
         const int tid_l = opaque(tid);
         const bool ok = mbar_wait_bounded(full, parity);
-        if (group_vote_or(bar, !ok)) {
-            if ((tid & 255) == 0) atomicOr(err, 1);
+        if (group_vote_or(bar, !ok, GS)) {
+            if (tid % GS == 0) atomicOr(err, 1);
             break;
         }
         const BatchSlot s = *slot;
         if (s.sq == BATCH_END) break;
         const BatchSquare& b = sq[s.sq];
         if (producer) {
-#define ZB_STORE(L) tma_store_even<TPlan<L>>(stage, &b.even_map, s.tile)
+#define ZB_STORE(L) tma_store_even<TPlan<L, LEPT>>(stage, &b.even_map, s.tile)
             ZB_BATCH_SWITCH(s.log_s, ZB_STORE)
 #undef ZB_STORE
         }
@@ -663,12 +670,12 @@ __global__ void __launch_bounds__(512, 1)
         // refills staging while everybody computes
 #define ZB_TILE(L)                                                                               \
     {                                                                                            \
-        using TP = TPlan<L>;                                                                     \
-        const Coords<TP> c(tid_l & 255, grp);                                                    \
-        uint2* xg = reinterpret_cast<uint2*>(smem + BATCH_OFF_X + (tid_l >> 8) * BATCH_X_BYTES); \
+        using TP = TPlan<L, LEPT>;                                                               \
+        const Coords<TP> c(tid_l % GS, grp);                                                     \
+        uint2* xg = reinterpret_cast<uint2*>(smem + BG::OFF_X + (tid_l / GS) * BG::X_BYTES);     \
         stage_read<TP>(v, smem, c);                                                              \
-        group_bar(bar);                                                                          \
-        if ((tid & 255) == 0) mbar_arrive(empty);                                                \
+        group_bar(bar, GS);                                                                      \
+        if (tid % GS == 0) mbar_arrive(empty);                                                   \
         if (producer) {                                                                          \
             const bool e_ok = mbar_wait_bounded(empty, parity);                                  \
             bulk_wait_read0();                                                                   \
@@ -682,7 +689,7 @@ __global__ void __launch_bounds__(512, 1)
         ZB_BATCH_SWITCH(s.log_s, ZB_TILE)
 #undef ZB_TILE
     }
-    if (stagger_pending) asm volatile("bar.arrive 3, 512;" ::: "memory");
+    stagger_release<BG::THREADS>(stagger_pending);
     if (producer) bulk_wait0();
 }
 

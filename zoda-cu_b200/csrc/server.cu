@@ -179,6 +179,7 @@ bool admit_and_launch(zoda_server* s, Slot& sl) {
     std::stable_sort(take.begin(), take.end(), [&](uint64_t a, uint64_t b) { return s->reqs[a].k > s->reqs[b].k; });
     uint64_t first = 0;
     uint32_t n = 0;
+    int max_log = 0;  // the launch's largest side sets its level radix
     const auto now = clk::now();
     for (uint64_t id : take) {
         Request& r = s->reqs[id];
@@ -196,6 +197,7 @@ bool admit_and_launch(zoda_server* s, Slot& sl) {
         }
         b.first = first;
         first += b.ntiles;
+        if (ls > max_log) max_log = ls;
         r.state = RState::Launched;
         sl.reqs.push_back(id);
         n++;
@@ -208,8 +210,11 @@ bool admit_and_launch(zoda_server* s, Slot& sl) {
     if (e == cudaSuccess) e = cudaMemsetAsync(sl.d_counter.p, 0, sizeof(unsigned long long), sl.st);
     zoda_status ls = ZODA_ERR_CUDA;
     if (e == cudaSuccess)
+    {
+        const int lept = batch_lept(s->ctx, max_log);
         ls = launch_batch_kernel(s->ctx, (const BatchSquare*)sl.d_sq.p, n, first, (unsigned long long*)sl.d_counter.p,
-                                 (const SideTables*)s->d_tables.p, sl.st);
+                                 (const SideTables*)s->d_tables.p + (lept == 3 ? 13 : 0), lept, sl.st);
+    }
     if (ls == ZODA_OK) e = cudaEventRecord(sl.done, sl.st);
     if (ls != ZODA_OK || e != cudaSuccess) {
         if (e != cudaSuccess) set_last_error("serving launch setup", e);
@@ -275,10 +280,13 @@ zoda_status zoda_server_create(zoda_ctx* ctx, const zoda_server_config* cfg, zod
     zoda_status st;
     if ((st = s->arena_mem.ensure(s->budget)) != ZODA_OK) return fail(st);
     s->arena.init(s->budget);
-    if ((st = s->d_tables.ensure(13 * sizeof(SideTables))) != ZODA_OK) return fail(st);
-    std::vector<SideTables> tabs(13);
-    for (int ls = BATCH_MIN_LOG; ls <= BATCH_MAX_LOG; ls++) tabs[ls] = side_tables(ctx, ls);
-    if ((e = cudaMemcpy(s->d_tables.p, tabs.data(), 13 * sizeof(SideTables), cudaMemcpyHostToDevice)) !=
+    if ((st = s->d_tables.ensure(26 * sizeof(SideTables))) != ZODA_OK) return fail(st);
+    std::vector<SideTables> tabs(26);  // radix 16 at [log_s], radix 8 at [13 + log_s]
+    for (int ls = BATCH_MIN_LOG; ls <= BATCH_MAX_LOG; ls++) {
+        tabs[ls] = side_tables(ctx, ls, 4);
+        tabs[13 + ls] = side_tables(ctx, ls, 3);
+    }
+    if ((e = cudaMemcpy(s->d_tables.p, tabs.data(), 26 * sizeof(SideTables), cudaMemcpyHostToDevice)) !=
         cudaSuccess) {
         set_last_error("cudaMemcpy(server tables)", e);
         return fail(ZODA_ERR_CUDA);

@@ -82,8 +82,12 @@ namespace zb {
 // Descriptor of one square; ZODA_ERR_UNSUPPORTED outside sides 32..2048.
 zoda_status make_batch_square(const zoda_square& q, BatchSquare* out, int promo = 3);
 // One launch of k_extend_batch over d_sq[0..nsq) (sorted by first), with
-// *d_counter already zero on `st`.
+// *d_counter already zero on `st`; d_tables[log_s] must hold the level tables
+// of radix 2^lept (4 or 3).
 zoda_status launch_batch_kernel(const zoda_ctx* ctx, const BatchSquare* d_sq, uint32_t nsq, uint64_t total_tiles,
-                                unsigned long long* d_counter, const SideTables* d_tables, cudaStream_t st);
+                                unsigned long long* d_counter, const SideTables* d_tables, int lept, cudaStream_t st);
 zoda_status set_batch_kernel_attributes();
+// The level radix a batch whose largest square has side 2^max_log uses: that
+// side's planned radix (it carries most of the bytes), else 16.
+int batch_lept(const zoda_ctx* ctx, int max_log);
 }  // namespace zb
