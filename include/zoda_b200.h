@@ -151,14 +151,14 @@ zoda_status zoda_ctx_check(zoda_ctx* ctx);
 zoda_status zoda_extend_device(zoda_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t k, uint64_t cols,
                                void* stream);
 
-/* Timing of a host-buffer call, in milliseconds (CUDA events). The copies
- * and kernels of different column chunks overlap, so the three busy times
- * can add up to more than total_ms. */
+/* Timing of a host-buffer call, in milliseconds. The copies and kernels of
+ * different column chunks overlap, so the three busy times (CUDA events) can
+ * add up to more than total_ms. */
 typedef struct zoda_timing {
-    float h2d_ms;    /* host -> device copies of the input, summed  */
-    float kernel_ms; /* fused extension kernels, summed             */
-    float d2h_ms;    /* device -> host copies of the output, summed */
-    float total_ms;  /* first copy start to last copy end           */
+    float h2d_ms;    /* host -> device copies of the input, summed          */
+    float kernel_ms; /* fused extension kernels, summed                     */
+    float d2h_ms;    /* device -> host copies of the odd output rows, summed */
+    float total_ms;  /* the whole call, host wall clock                     */
 } zoda_timing;
 
 /* Fused extension from host memory to host memory: the reference's
@@ -167,7 +167,9 @@ typedef struct zoda_timing {
  * [k][cols], h_out row-major [2k][cols]; pinned buffers give full PCIe speed.
  * The square moves in column chunks over three streams, so uploads,
  * kernels and downloads overlap; device buffers are the context's cached
- * chunk buffers. Synchronous. `timing` may be NULL. */
+ * chunk buffers. Only the odd output rows cross PCIe: the even rows equal the
+ * input rows and host threads copy them meanwhile. Synchronous. `timing` may
+ * be NULL. */
 zoda_status zoda_extend_host(zoda_ctx* ctx, const uint32_t* h_in, uint32_t* h_out, uint32_t k, uint64_t cols,
                              zoda_timing* timing);
 

@@ -136,15 +136,26 @@ def test_extend_erasure_recovery(ctx):
     assert np.array_equal(rec, data)
 
 
-@pytest.mark.parametrize("side,cols", [(256, 4096), (512, 512 * 128 + 4 * 37)])
+@pytest.mark.parametrize("side,cols", [(1, 64), (2, 128), (16, 2048 + 4), (256, 4096), (512, 512 * 128 + 4 * 37),
+                                       (2048, 4096), (4096, 256)])
 def test_extend_host_matches_device(ctx, side, cols):
-    # the second case moves ~134 MB in three column chunks over three streams, the last one ragged
+    # (512, ...) moves ~134 MB in three column chunks over three streams, the last one ragged;
+    # only the odd rows come back over PCIe, the even rows are copied on the host
     data = O.seeded_input(side, cols, seed=9)
     h_in = torch.from_numpy(data.view(np.int32)).pin_memory()
-    h_out = torch.empty((2 * side, cols), dtype=torch.int32).pin_memory()
+    h_out = torch.full((2 * side, cols), -1, dtype=torch.int32).pin_memory()
     t = ctx.extend_host(h_in, h_out, side, cols)
     assert t.kernel_ms > 0 and t.total_ms >= t.kernel_ms
     assert np.array_equal(h_out.numpy().view(np.uint32), run_extend(ctx, data))
+
+
+def test_extend_host_pageable_buffers(ctx):
+    side, cols = 128, 128 * 128
+    data = O.seeded_input(side, cols, seed=13)
+    h_in = torch.from_numpy(data.view(np.int32).copy())  # not pinned
+    h_out = torch.full((2 * side, cols), -1, dtype=torch.int32)
+    ctx.extend_host(h_in, h_out, side, cols)
+    assert np.array_equal(h_out.numpy().view(np.uint32), O.encode_rowmajor(data))
 
 
 def test_extend_rejects_bad_arguments(ctx):

@@ -6,13 +6,14 @@
 namespace zb {
 
 namespace {
-// S = 1: NTT_2 of (v, 0) is (v, v).
-__global__ void k_extend_side1(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint64_t cols) {
+// S = 1: NTT_2 of (v, 0) is (v, v); with odd_only just the odd row.
+__global__ void k_extend_side1(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint64_t cols,
+                               bool odd_only) {
     for (uint64_t c = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) * 4; c < cols;
          c += (uint64_t)gridDim.x * blockDim.x * 4) {
         V4 x = ld_v4(in + c);
         st_v4(out + c, x);
-        st_v4(out + cols + c, x);
+        if (!odd_only) st_v4(out + cols + c, x);
     }
 }
 
@@ -138,12 +139,12 @@ int side_l2_promo(const zoda_ctx* ctx, int log_s) {
 }
 
 zoda_status launch_plan(const zoda_ctx* ctx, int log_s, const zoda_plan& p, const uint32_t* in, uint32_t* out,
-                        uint64_t cols, cudaStream_t st) {
+                        uint64_t cols, cudaStream_t st, bool odd_only) {
     zoda_status s = check_plan(log_s, p);
     if (s != ZODA_OK) return s;
     // stagger 1: release after all INTT levels but the last; 2: after the first; 3: right away
     const uint32_t at_code = p.stagger == 2 ? 2u : p.stagger == 3 ? 1u : 0u;
-    const uint32_t flags = (p.blocked ? 1u : 0u) | (p.stagger ? 0u : 2u) | (at_code << 2);
+    const uint32_t flags = (p.blocked ? 1u : 0u) | (p.stagger ? 0u : 2u) | (at_code << 2) | (odd_only ? 16u : 0u);
     if (p.impl == ZODA_IMPL_TMA) {
         switch (log_s) {
 #define ZB_CASE(L)                                                                  \
@@ -159,7 +160,7 @@ zoda_status launch_plan(const zoda_ctx* ctx, int log_s, const zoda_plan& p, cons
         case 0: {
             const uint64_t quads = cols / 4;
             const unsigned grid = (unsigned)((quads + 255) / 256 < 4096 ? (quads + 255) / 256 : 4096);
-            if (grid) k_extend_side1<<<grid, 256, 0, st>>>(in, out, cols);
+            if (grid) k_extend_side1<<<grid, 256, 0, st>>>(in, out, cols, odd_only);
             ZB_CUDA(cudaGetLastError());
             return ZODA_OK;
         }
@@ -173,13 +174,13 @@ zoda_status launch_plan(const zoda_ctx* ctx, int log_s, const zoda_plan& p, cons
 }
 
 zoda_status launch_extend(const zoda_ctx* ctx, int log_s, const uint32_t* in, uint32_t* out, uint64_t cols,
-                          cudaStream_t st, int impl) {
+                          cudaStream_t st, int impl, bool odd_only) {
     if (log_s < 0 || log_s > 12) return ZODA_ERR_UNSUPPORTED;
     zoda_plan p = default_plan(log_s);
     if (impl == ZODA_IMPL_AUTO && ctx->planned[log_s]) p = ctx->plan[log_s];
     else if (impl == ZODA_IMPL_DIRECT) p.impl = ZODA_IMPL_DIRECT;
     else if (impl == ZODA_IMPL_TMA) p.impl = ZODA_IMPL_TMA;
-    return launch_plan(ctx, log_s, p, in, out, cols, st);
+    return launch_plan(ctx, log_s, p, in, out, cols, st, odd_only);
 }
 
 }  // namespace zb

@@ -157,15 +157,18 @@ __device__ __forceinline__ void dif_levels(V4* v, uint4* sm, int t, int q, const
 }
 
 template <class PL, int l>
-__device__ __forceinline__ void ntt_levels(V4* v, uint4* sm, int t, int q, const Tw* tw, uint32_t* __restrict__ out,
-                                           uint64_t cols, uint64_t col, bool active) {
+// Odd output row k goes to out_odd + k * ostride (out + cols, 2 * cols for the
+// interleaved [2S][cols] layout; out, cols for odd rows only).
+__device__ __forceinline__ void ntt_levels(V4* v, uint4* sm, int t, int q, const Tw* tw,
+                                           uint32_t* __restrict__ out_odd, uint64_t ostride, uint64_t col,
+                                           bool active) {
     using LV = Level<PL, PL::nlr(l), PL::npre(l)>;
     if constexpr (l > 0) LV::read(v, sm, t, q);
     LV::template dft<false>(v);
     if constexpr (l < PL::NLEV - 1) {
         LV::template twiddle_write<false>(v, sm, t, q, tw);
         __syncthreads();
-        ntt_levels<PL, l + 1>(v, sm, t, q, tw, out, cols, col, active);
+        ntt_levels<PL, l + 1>(v, sm, t, q, tw, out_odd, ostride, col, active);
     } else {
         // last level: L = 1, slot = block*R + k2 -> output index by digit reversal
 #pragma unroll
@@ -174,7 +177,7 @@ __device__ __forceinline__ void ntt_levels(V4* v, uint4* sm, int t, int q, const
 #pragma unroll
             for (int r = 0; r < LV::R; r++) {
                 const uint32_t k = digit_rev<PL, true>((blk << PL::nlr(l)) + (uint32_t)bitrev(r, PL::nlr(l)));
-                if (active) stg_stream_v4(out + (2 * (uint64_t)k + 1) * cols + col, v[g * LV::R + r]);
+                if (active) stg_stream_v4(out_odd + (uint64_t)k * ostride + col, v[g * LV::R + r]);
             }
         }
     }
@@ -187,8 +190,8 @@ __device__ __forceinline__ void ntt_levels(V4* v, uint4* sm, int t, int q, const
 // coefficients, in natural k2 order, as group n1 = c0.
 template <class PL>
 __device__ __forceinline__ void twist_and_first_ntt(V4* v, uint4* sm, int t, int q, const Tw* tw,
-                                                    const Tw* __restrict__ twist, uint32_t* __restrict__ out,
-                                                    uint64_t cols, uint64_t col, bool active) {
+                                                    const Tw* __restrict__ twist, uint32_t* __restrict__ out_odd,
+                                                    uint64_t ostride, uint64_t col, bool active) {
     constexpr int LR = PL::lr(PL::NLEV - 1);
     constexpr int R = 1 << LR;
     constexpr int G = PL::EPT / R;
@@ -224,13 +227,13 @@ __device__ __forceinline__ void twist_and_first_ntt(V4* v, uint4* sm, int t, int
             }
         }
         __syncthreads();
-        ntt_levels<PL, 1>(v, sm, t, q, tw, out, cols, col, active);
+        ntt_levels<PL, 1>(v, sm, t, q, tw, out_odd, ostride, col, active);
     } else {
         // single level: output index k2 = bitrev(r)
 #pragma unroll
         for (int r = 0; r < R; r++) {
             const uint32_t k = (uint32_t)bitrev(r, LR);
-            if (active) stg_stream_v4(out + (2 * (uint64_t)k + 1) * cols + col, v[r]);
+            if (active) stg_stream_v4(out_odd + (uint64_t)k * ostride + col, v[r]);
         }
     }
 }
@@ -267,6 +270,10 @@ __global__ void __launch_bounds__(LEPT == 3 ? 1024 : 512, 1)
     const int t = tid / PL::Q4;
     const Tw* twist = twist_all + PL::S;  // g^i / S for this side, i in [0, S)
     V4 v[PL::EPT];
+    // flags bit 4: write only the odd rows, compactly (out is then [S][cols])
+    const bool odd_only = flags & 16;
+    uint32_t* const out_odd = odd_only ? out : out + cols;
+    const uint64_t ostride = odd_only ? cols : 2 * cols;
     const TileRange tr(ntiles, flags & 1);
     for (uint64_t tile = tr.first; tile < tr.last; tile += tr.step) {
         const uint64_t col = tile * PL::C + 4 * (uint64_t)q;
@@ -284,13 +291,13 @@ __global__ void __launch_bounds__(LEPT == 3 ? 1024 : 512, 1)
                 const uint64_t row = (uint64_t)(g * PL::TPQ + t) + (uint64_t)L0 * j;
                 if (active) {
                     v[g * R0 + j] = ldg_stream_v4(in + row * cols + col);
-                    stg_stream_v4(out + 2 * row * cols + col, v[g * R0 + j]);
+                    if (!odd_only) stg_stream_v4(out + 2 * row * cols + col, v[g * R0 + j]);
                 } else {
                     v[g * R0 + j] = V4{{0, 0, 0, 0}};
                 }
             }
         dif_levels<PL, 0, true>(v, sm, t, q, tw);
-        twist_and_first_ntt<PL>(v, sm, t, q, tw, twist, out, cols, col, active);
+        twist_and_first_ntt<PL>(v, sm, t, q, tw, twist, out_odd, ostride, col, active);
     }
 }
 

@@ -347,7 +347,8 @@ __device__ __forceinline__ void intt_upto_last(V4* v, uint2* xg, int t, int ql, 
 // the odd output rows.
 template <class TP, int l>
 __device__ __forceinline__ void ntt_from(V4* v, uint2* xg, int t, int ql, int bar, const SideTables& tb,
-                                         uint32_t* __restrict__ out, uint64_t cols, uint64_t col, bool active) {
+                                         uint32_t* __restrict__ out_odd, uint64_t ostride, uint64_t col,
+                                         bool active) {
     using LV = LvlGeom<TP, TP::nlr(l), TP::npre(l)>;
     if constexpr (l < TP::NLEV - 1) {
         using Rd = LvlGeom<TP, TP::nlr(l + 1), TP::npre(l + 1)>;
@@ -359,7 +360,7 @@ __device__ __forceinline__ void ntt_from(V4* v, uint2* xg, int t, int ql, int ba
         exchange<TP, LV::R, LV::LOGL, Rd::R, Rd::LOGL>(
             v, xg, ql, bar, [&](int g) { return LV::base(LV::gid(g, t)); },
             [&](int g) { return Rd::base(Rd::gid(g, t)); });
-        ntt_from<TP, l + 1>(v, xg, t, ql, bar, tb, out, cols, col, active);
+        ntt_from<TP, l + 1>(v, xg, t, ql, bar, tb, out_odd, ostride, col, active);
     } else {
 #pragma unroll
         for (int g = 0; g < LV::G; g++) dft_dif<TP::nlr(l), false>(v + g * LV::R);
@@ -370,7 +371,7 @@ __device__ __forceinline__ void ntt_from(V4* v, uint2* xg, int t, int ql, int ba
             for (int r = 0; r < LV::R; r++) {
                 const uint32_t k =
                     digit_rev<typename TP::PL, true>((blk << TP::nlr(l)) | (uint32_t)bitrev(r, TP::nlr(l)));
-                if (active) stg_stream_v4(out + (2 * (uint64_t)k + 1) * cols + col, v[g * LV::R + r]);
+                if (active) stg_stream_v4(out_odd + (uint64_t)k * ostride + col, v[g * LV::R + r]);
             }
         }
     }
@@ -418,12 +419,13 @@ __device__ __forceinline__ void stage_read(V4* v, const unsigned char* smem, con
     }
 }
 
-// Everything after the tile is in registers: INTT, twist, NTT, odd-row stores.
+// Everything after the tile is in registers: INTT, twist, NTT, odd-row stores
+// (odd row k at out_odd + k * ostride).
 // With stagger_pending set, group 0 releases group 1 (named barrier 3) when it
 // starts INTT level stagger_at (NLEV-1: after all INTT levels but the last).
 template <class TP>
 __device__ __forceinline__ void tile_compute(V4* v, uint2* xg, const Coords<TP>& c, int bar, const SideTables& tb,
-                                             uint32_t* __restrict__ out, uint64_t cols, uint64_t col, bool active,
+                                             uint32_t* __restrict__ out_odd, uint64_t ostride, uint64_t col, bool active,
                                              bool& stagger_pending, int stagger_at = TP::NLEV - 1) {
     const int t = c.t, ql = c.ql;
     // ---- INTT levels 0 .. NLEV-2
@@ -458,7 +460,7 @@ __device__ __forceinline__ void tile_compute(V4* v, uint2* xg, const Coords<TP>&
             [&](int g) { return Rd::base(Rd::gid(g, t)); });
     }
     // ---- NTT levels 1 .. NLEV-1, the last one stores the odd rows
-    ntt_from<TP, 1>(v, xg, t, ql, bar, tb, out, cols, col, active);
+    ntt_from<TP, 1>(v, xg, t, ql, bar, tb, out_odd, ostride, col, active);
 }
 
 // Re-derive a value from an opaque copy so the compiler rebuilds per-tile
@@ -472,7 +474,8 @@ __device__ __forceinline__ int opaque(int x) {
 // ---- one square ------------------------------------------------------------------
 // flags: bit 0 = blocked tile order (TileRange), bit 1 = no stagger between the
 // warp-groups, bits 2-3 = the INTT level at which group 0 releases group 1,
-// plus one (0: the default, after all INTT levels but the last).
+// plus one (0: the default, after all INTT levels but the last), bit 4 = write
+// only the odd rows, compactly ([S][cols]; the even rows are the input).
 template <int LOG_S, int LEPT = 4>
 __global__ void __launch_bounds__(TPlan<LOG_S, LEPT>::THREADS, 1)
     k_extend_tma(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_even,
@@ -497,6 +500,9 @@ __global__ void __launch_bounds__(TPlan<LOG_S, LEPT>::THREADS, 1)
     __syncthreads();
     const TileRange tr(ntiles, flags & 1);
     const bool stagger = !(flags & 2);
+    const bool odd_only = flags & 16;  // only the odd rows, compactly: out is then [S][cols]
+    uint32_t* const out_odd = odd_only ? out : out + cols;
+    const uint64_t ostride = odd_only ? cols : 2 * cols;
     const int stagger_at = (flags >> 2) & 3 ? (int)((flags >> 2) & 3) - 1 : TP::NLEV - 1;
     uint64_t tile = tr.first;
     if (producer && tile < tr.last) tma_load_tile<TP>(stage, &tm_in, tile, full);
@@ -517,7 +523,7 @@ __global__ void __launch_bounds__(TPlan<LOG_S, LEPT>::THREADS, 1)
             if (producer) bulk_wait0();
             return;
         }
-        if (producer) tma_store_even<TP>(stage, &tm_even, tile);  // even output rows = the input tile
+        if (producer && !odd_only) tma_store_even<TP>(stage, &tm_even, tile);  // even output rows = the input tile
         const uint64_t col = tile * TP::C + 4 * (uint64_t)c.q;
         const bool active = col < cols;
         stage_read<TP>(v, smem, c);
@@ -531,7 +537,7 @@ __global__ void __launch_bounds__(TPlan<LOG_S, LEPT>::THREADS, 1)
             if (e_ok) tma_load_tile<TP>(stage, &tm_in, next, full);
             else atomicOr(err, 2);  // both groups then time out on `full` and leave
         }
-        tile_compute<TP>(v, xg, c, bar, tb, out, cols, col, active, stagger_pending, stagger_at);
+        tile_compute<TP>(v, xg, c, bar, tb, out_odd, ostride, col, active, stagger_pending, stagger_at);
     }
     stagger_release<TP::THREADS>(stagger_pending);
     if (producer) bulk_wait0();
@@ -684,7 +690,7 @@ __global__ void __launch_bounds__(BatchGeom<LEPT>::THREADS, 1)
             else atomicOr(err, 2);                                                               \
         }                                                                                        \
         const uint64_t col = s.tile * TP::C + 4 * (uint64_t)c.q;                                 \
-        tile_compute<TP>(v, xg, c, bar, tb, out, cols, col, col < cols, stagger_pending);        \
+        tile_compute<TP>(v, xg, c, bar, tb, out + cols, 2 * cols, col, col < cols, stagger_pending); \
     }
         ZB_BATCH_SWITCH(s.log_s, ZB_TILE)
 #undef ZB_TILE

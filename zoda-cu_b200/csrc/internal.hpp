@@ -80,16 +80,17 @@ struct zoda_ctx {
 namespace zb {
 // Launches the fused extension kernel for side 2^log_s (0 <= log_s <= 12).
 // impl: 0 = the side's plan (tuned, or the default), 1 = direct-load kernel,
-// 2 = TMA-staged kernel (sides 32..4096), both with default knobs.
+// 2 = TMA-staged kernel (sides 32..4096), both with default knobs. With
+// odd_only the kernel writes only the odd rows, as a compact [S][cols] out.
 zoda_status launch_extend(const zoda_ctx* ctx, int log_s, const uint32_t* in, uint32_t* out, uint64_t cols,
-                          cudaStream_t st, int impl = 0);
+                          cudaStream_t st, int impl = 0, bool odd_only = false);
 // The plan a side runs with impl 0 and no tuning.
 zoda_plan default_plan(int log_s);
 // ZODA_OK when the plan can run for this side.
 zoda_status check_plan(int log_s, const zoda_plan& p);
 // Launches one explicit plan.
 zoda_status launch_plan(const zoda_ctx* ctx, int log_s, const zoda_plan& p, const uint32_t* in, uint32_t* out,
-                        uint64_t cols, cudaStream_t st);
+                        uint64_t cols, cudaStream_t st, bool odd_only = false);
 // The L2 promotion a side's TMA loads use on this context (for the batch maps).
 int side_l2_promo(const zoda_ctx* ctx, int log_s);
 // Sets the dynamic shared memory attribute of every extension instantiation.
