@@ -155,3 +155,26 @@ def test_legacy_matches_reference_cuda_kernel(zb, log_n, inverse):
     assert fn(a.ctypes.data, roots.ctypes.data, n, polys, stride) == 0
     (zb.intt_cuda if inverse else zb.ntt_cuda)(b, n, stride)
     assert np.array_equal(a, b)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SO), reason="reference CUDA build not present")
+@pytest.mark.parametrize("side,cols", [(64, 8192), (1024, 2048)])
+def test_fused_extension_matches_reference_cuda_encode(zb, side, cols):
+    """The reference's GPU encode window (src/benchmarks/utils.rs:114-140: column-major
+    square, zero rows k..2k, intt_cuda over k rows, ntt_cuda over 2k) run by the reference's
+    own CUDA kernel, against the fused extension kernel, on the same seeded input."""
+    import torch
+    ref = ctypes.CDLL(REF_SO)
+    ref.cuda_ntt.argtypes = ref.cuda_intt.argtypes = [ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_uint32] * 3
+    data = O.seeded_input(side, cols, seed=side + 7)
+    square = np.zeros((cols, 2 * side), dtype=np.uint32)  # column c at square[c]
+    square[:, :side] = data.T
+    assert ref.cuda_intt(square.ctypes.data, O.roots_of_unity(side).ctypes.data, side, cols, 2 * side) == 0
+    assert ref.cuda_ntt(square.ctypes.data, O.roots_of_unity(2 * side).ctypes.data, 2 * side, cols, 2 * side) == 0
+    ctx = zb.Context(0)
+    d_in = torch.from_numpy(data.view(np.int32)).cuda()
+    d_out = torch.empty((2 * side, cols), dtype=torch.int32, device="cuda")
+    ctx.extend(d_in, d_out, side, cols)
+    torch.cuda.synchronize()
+    ctx.close()
+    assert np.array_equal(d_out.cpu().numpy().view(np.uint32), square.T)
