@@ -326,7 +326,7 @@ zoda_status zoda_rlc_coefficients_device(zoda_ctx* ctx, const char* root, size_t
                                          uint32_t* d_coeff, void* stream);
 
 /* rlc_row (src/zoda/rlc.rs:32-40) for every row: d_out[4*r + l] =
- * sum_c d_rows[r*cols + c] * d_coeff[4*c + l] mod p, rows < 524288.
+ * sum_c d_rows[r*cols + c] * d_coeff[4*c + l] mod p, rows <= 262140.
  * One HBM read of the matrix. Asynchronous. */
 zoda_status zoda_rlc_rows_device(zoda_ctx* ctx, const uint32_t* d_rows, uint32_t rows, uint64_t cols,
                                  const uint32_t* d_coeff, uint32_t* d_out, void* stream);

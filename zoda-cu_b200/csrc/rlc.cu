@@ -255,7 +255,7 @@ zoda_status rlc_rows(const zoda_ctx* ctx, const uint32_t* x, uint32_t rows, uint
     uint64_t gx = (quads + 256 * 8 - 1) / (256 * 8) * (8 / RB);  // ~RB column quads per thread
     if (gx < 1) gx = 1;
     if (gy > 65535) {
-        set_last_error_text("rlc: more than 524280 rows");
+        set_last_error_text("rlc: more than 262140 rows");
         return ZODA_ERR_UNSUPPORTED;
     }
     if (quads) {
