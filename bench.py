@@ -321,7 +321,7 @@ def time_encode_general(ctx, k: int, n: int, reps: int = 5) -> dict:
     torch.cuda.empty_cache()
     return {"k": k, "n": n, "cols": cols, "ms": round(ms, 4),
             "gbps": round(k * k * 512 * 8.0 / (ms * 1e-3) / 1e9, 1), "data_rows_ok": ok,
-            "api": "zoda_encode_device (interpolate over next_pow2(k), one evaluation per coset)"}
+            "api": "zoda_encode_device (n_kn = 2 n_k: the fused kernels, zeros past row k, output cut at k+n)"}
 
 
 def time_device_extend(ctx, side: int, steps: int, warmup: int, world: int, sampler=None):

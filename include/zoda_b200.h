@@ -286,8 +286,9 @@ void zoda_server_destroy(zoda_server* srv);
  * omega_{n_kn}^j; d_out receives rows j = 0 .. k+n-1 (the encoded_rows of
  * utils.rs:167-168), row-major [k+n][cols]. d_in is row-major [k][cols].
  * Limits: next_pow2(k) <= 4096, k + n <= 2^27, cols % 4 == 0, 16-byte aligned
- * buffers that do not overlap. n == k with k a power of two is exactly
- * zoda_extend_device; every other shape runs one interpolation and one
+ * buffers that do not overlap. When n_kn = 2 n_k (n <= 2 n_k - k, e.g. any
+ * k = n) the fused extension kernels run it in one pass, as zoda_extend_device
+ * does for power-of-two squares; other shapes run one interpolation and one
  * evaluation per coset on the general column transform, in column chunks
  * whose scratch (<= 256 MiB) the context keeps. Asynchronous on `stream`. */
 zoda_status zoda_encode_device(zoda_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t k, uint32_t n,

@@ -48,12 +48,20 @@ SHAPES = [
     (1000, 1000), # n_k 1024, n_kn 2048
     (3, 125),     # rate 1/32
     (2048, 100),  # n_k 2048, n_kn 4096
+    (3, 3),       # n_k 4, n_kn 8, fused kernels with rows cut
+    (2, 1),       # n_k 2, n_kn 4
+    (33, 31),     # n_k 64, fused, 64 output rows
+    (300, 212),   # n_k 512, fused, n_kn 1024 exactly filled
+    (1500, 1000), # n_k 2048, fused with the tuned side-2048 plan
+    (3000, 3000), # n_k 4096, fused (direct kernel)
 ]
 
 
 @pytest.mark.parametrize("k,n", SHAPES, ids=[f"k{k}-n{n}" for k, n in SHAPES])
 def test_encode_any_shape_matches_oracle(ctx, k, n):
     cols = 36 if k >= 1000 else 2 * 2048 + 20
+    if (k, n) in ((33, 31), (300, 212)):
+        cols = 3 * 32768 // 64 + 12 if k == 33 else 3 * 64 + 12  # several tiles, ragged
     data = O.seeded_input(k, cols, seed=7 * k + n)
     want = O.encode_rowmajor(data, n)
     d_in = to_dev(data)
@@ -79,8 +87,9 @@ def test_encode_square_power_of_two_is_the_extension(ctx):
 
 
 def test_encode_many_column_chunks(ctx):
-    # n_k = 4096, n_kn = 8192, with more columns than one 256 MiB scratch chunk holds (16384)
-    k, n, cols = 3000, 3000, 16384 + 64
+    # n_k = 4096, n_kn = 16384 (the interpolation + per-coset path), with more columns than one
+    # 256 MiB scratch chunk holds (16384)
+    k, n, cols = 3000, 9000, 16384 + 64
     data = O.seeded_input(k, cols, seed=11)
     d_in = to_dev(data)
     d_out = torch.empty((k + n, cols), dtype=torch.int32, device="cuda")

@@ -19,31 +19,31 @@ __global__ void k_extend_side1(const uint32_t* __restrict__ in, uint32_t* __rest
 
 template <int LOG_S, int SCHED, int LEPT = 4>
 zoda_status launch_t(const zoda_ctx* ctx, const uint32_t* in, uint32_t* out, uint64_t cols, uint32_t flags,
-                     cudaStream_t st) {
+                     uint32_t in_rows, uint32_t out_rows, cudaStream_t st) {
     using PL = ExtPlan<LOG_S, SCHED, LEPT, LEPT == 3 ? 1024 : 512>;
     const uint64_t ntiles = (cols + PL::C - 1) / PL::C;
     if (ntiles == 0) return ZODA_OK;
     const uint64_t grid = ntiles < (uint64_t)ctx->sm_count ? ntiles : (uint64_t)ctx->sm_count;
     k_extend<LOG_S, SCHED, LEPT><<<(unsigned)grid, PL::THREADS, PL::SMEM, st>>>(in, out, cols, ntiles,
                                                                                 ctx->tables.tw, ctx->tables.twist,
-                                                                                flags);
+                                                                                flags, in_rows, out_rows);
     ZB_CUDA(cudaGetLastError());
     return ZODA_OK;
 }
 
 template <int LOG_S, int LEPT>
 zoda_status launch_tma_t(const zoda_ctx* ctx, const uint32_t* in, uint32_t* out, uint64_t cols, int promo,
-                         uint32_t flags, cudaStream_t st) {
+                         uint32_t flags, uint32_t in_rows, uint32_t out_rows, cudaStream_t st) {
     using TP = TPlan<LOG_S, LEPT>;
     const uint64_t ntiles = (cols + TP::C - 1) / TP::C;
     if (ntiles == 0) return ZODA_OK;
     CUtensorMap m_in, m_even;
-    zoda_status s = make_tile_maps<TP>(&m_in, &m_even, in, out, cols, promo);
+    zoda_status s = make_tile_maps<TP>(&m_in, &m_even, in, out, cols, promo, in_rows, (out_rows + 1) / 2);
     if (s != ZODA_OK) return s;
     const uint64_t grid = ntiles < (uint64_t)ctx->sm_count ? ntiles : (uint64_t)ctx->sm_count;
     const SideTables tb = side_tables(ctx, LOG_S, LEPT);
     k_extend_tma<LOG_S, LEPT><<<(unsigned)grid, TP::THREADS, TP::SMEM, st>>>(m_in, m_even, out, cols, ntiles, tb,
-                                                                            ctx->d_err, flags);
+                                                                            ctx->d_err, flags, out_rows);
     ZB_CUDA(cudaGetLastError());
     return ZODA_OK;
 }
@@ -82,17 +82,17 @@ zoda_status set_attr_t() {
 
 template <int LOG_S>
 zoda_status launch_direct(const zoda_ctx* ctx, int sched, int radix, const uint32_t* in, uint32_t* out,
-                          uint64_t cols, uint32_t flags, cudaStream_t st) {
+                          uint64_t cols, uint32_t flags, uint32_t in_rows, uint32_t out_rows, cudaStream_t st) {
     if constexpr (has_direct_r8(LOG_S)) {
         if (radix == 8) {
             if constexpr (has_sched1_r8(LOG_S))
-                if (sched == 1) return launch_t<LOG_S, 1, 3>(ctx, in, out, cols, flags, st);
-            return launch_t<LOG_S, 0, 3>(ctx, in, out, cols, flags, st);
+                if (sched == 1) return launch_t<LOG_S, 1, 3>(ctx, in, out, cols, flags, in_rows, out_rows, st);
+            return launch_t<LOG_S, 0, 3>(ctx, in, out, cols, flags, in_rows, out_rows, st);
         }
     }
     if constexpr (has_sched1(LOG_S))
-        if (sched == 1) return launch_t<LOG_S, 1>(ctx, in, out, cols, flags, st);
-    return launch_t<LOG_S, 0>(ctx, in, out, cols, flags, st);
+        if (sched == 1) return launch_t<LOG_S, 1>(ctx, in, out, cols, flags, in_rows, out_rows, st);
+    return launch_t<LOG_S, 0>(ctx, in, out, cols, flags, in_rows, out_rows, st);
 }
 }  // namespace
 
@@ -139,9 +139,13 @@ int side_l2_promo(const zoda_ctx* ctx, int log_s) {
 }
 
 zoda_status launch_plan(const zoda_ctx* ctx, int log_s, const zoda_plan& p, const uint32_t* in, uint32_t* out,
-                        uint64_t cols, cudaStream_t st, bool odd_only) {
+                        uint64_t cols, cudaStream_t st, bool odd_only, uint32_t in_rows, uint32_t out_rows) {
     zoda_status s = check_plan(log_s, p);
     if (s != ZODA_OK) return s;
+    const uint32_t S = 1u << log_s;
+    if (in_rows == 0) in_rows = S;
+    if (out_rows == 0) out_rows = 2 * S;
+    if (in_rows > S || out_rows > 2 * S || (log_s == 0 && (in_rows != 1 || out_rows != 2))) return ZODA_ERR_ARG;
     // stagger 1: release after all INTT levels but the last; 2: after the first; 3: right away
     const uint32_t at_code = p.stagger == 2 ? 2u : p.stagger == 3 ? 1u : 0u;
     const uint32_t flags = (p.blocked ? 1u : 0u) | (p.stagger ? 0u : 2u) | (at_code << 2) | (odd_only ? 16u : 0u);
@@ -149,8 +153,8 @@ zoda_status launch_plan(const zoda_ctx* ctx, int log_s, const zoda_plan& p, cons
         switch (log_s) {
 #define ZB_CASE(L)                                                                  \
     case L:                                                                         \
-        return p.radix == 8 ? launch_tma_t<L, 3>(ctx, in, out, cols, p.l2_promo, flags, st) \
-                            : launch_tma_t<L, 4>(ctx, in, out, cols, p.l2_promo, flags, st);
+        return p.radix == 8 ? launch_tma_t<L, 3>(ctx, in, out, cols, p.l2_promo, flags, in_rows, out_rows, st) \
+                            : launch_tma_t<L, 4>(ctx, in, out, cols, p.l2_promo, flags, in_rows, out_rows, st);
             ZB_CASE(5) ZB_CASE(6) ZB_CASE(7) ZB_CASE(8) ZB_CASE(9) ZB_CASE(10) ZB_CASE(11) ZB_CASE(12)
 #undef ZB_CASE
             default: return ZODA_ERR_UNSUPPORTED;
@@ -165,7 +169,7 @@ zoda_status launch_plan(const zoda_ctx* ctx, int log_s, const zoda_plan& p, cons
             return ZODA_OK;
         }
 #define ZB_CASE(L) \
-    case L: return launch_direct<L>(ctx, p.sched, p.radix, in, out, cols, flags, st);
+    case L: return launch_direct<L>(ctx, p.sched, p.radix, in, out, cols, flags, in_rows, out_rows, st);
         ZB_CASE(1) ZB_CASE(2) ZB_CASE(3) ZB_CASE(4) ZB_CASE(5) ZB_CASE(6)
         ZB_CASE(7) ZB_CASE(8) ZB_CASE(9) ZB_CASE(10) ZB_CASE(11) ZB_CASE(12)
 #undef ZB_CASE
@@ -174,13 +178,13 @@ zoda_status launch_plan(const zoda_ctx* ctx, int log_s, const zoda_plan& p, cons
 }
 
 zoda_status launch_extend(const zoda_ctx* ctx, int log_s, const uint32_t* in, uint32_t* out, uint64_t cols,
-                          cudaStream_t st, int impl, bool odd_only) {
+                          cudaStream_t st, int impl, bool odd_only, uint32_t in_rows, uint32_t out_rows) {
     if (log_s < 0 || log_s > 12) return ZODA_ERR_UNSUPPORTED;
     zoda_plan p = default_plan(log_s);
     if (impl == ZODA_IMPL_AUTO && ctx->planned[log_s]) p = ctx->plan[log_s];
     else if (impl == ZODA_IMPL_DIRECT) p.impl = ZODA_IMPL_DIRECT;
     else if (impl == ZODA_IMPL_TMA) p.impl = ZODA_IMPL_TMA;
-    return launch_plan(ctx, log_s, p, in, out, cols, st, odd_only);
+    return launch_plan(ctx, log_s, p, in, out, cols, st, odd_only, in_rows, out_rows);
 }
 
 }  // namespace zb

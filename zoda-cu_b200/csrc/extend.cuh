@@ -156,19 +156,26 @@ __device__ __forceinline__ void dif_levels(V4* v, uint4* sm, int t, int q, const
     }
 }
 
+// Where the odd output rows go: row k (k < rows) at p + k * stride, with
+// (out + cols, 2 * cols) for the interleaved [2S][cols] layout and (out, cols)
+// for the odd rows only; rows < S when the output is cut short (an encoding
+// with fewer parity rows than data rows).
+struct OddOut {
+    uint32_t* p;
+    uint64_t stride;
+    uint32_t rows;
+};
+
 template <class PL, int l>
-// Odd output row k goes to out_odd + k * ostride (out + cols, 2 * cols for the
-// interleaved [2S][cols] layout; out, cols for odd rows only).
 __device__ __forceinline__ void ntt_levels(V4* v, uint4* sm, int t, int q, const Tw* tw,
-                                           uint32_t* __restrict__ out_odd, uint64_t ostride, uint64_t col,
-                                           bool active) {
+                                           const OddOut& oo, uint64_t col, bool active) {
     using LV = Level<PL, PL::nlr(l), PL::npre(l)>;
     if constexpr (l > 0) LV::read(v, sm, t, q);
     LV::template dft<false>(v);
     if constexpr (l < PL::NLEV - 1) {
         LV::template twiddle_write<false>(v, sm, t, q, tw);
         __syncthreads();
-        ntt_levels<PL, l + 1>(v, sm, t, q, tw, out_odd, ostride, col, active);
+        ntt_levels<PL, l + 1>(v, sm, t, q, tw, oo, col, active);
     } else {
         // last level: L = 1, slot = block*R + k2 -> output index by digit reversal
 #pragma unroll
@@ -177,7 +184,7 @@ __device__ __forceinline__ void ntt_levels(V4* v, uint4* sm, int t, int q, const
 #pragma unroll
             for (int r = 0; r < LV::R; r++) {
                 const uint32_t k = digit_rev<PL, true>((blk << PL::nlr(l)) + (uint32_t)bitrev(r, PL::nlr(l)));
-                if (active) stg_stream_v4(out_odd + (uint64_t)k * ostride + col, v[g * LV::R + r]);
+                if (active && k < oo.rows) stg_stream_v4(oo.p + (uint64_t)k * oo.stride + col, v[g * LV::R + r]);
             }
         }
     }
@@ -190,8 +197,8 @@ __device__ __forceinline__ void ntt_levels(V4* v, uint4* sm, int t, int q, const
 // coefficients, in natural k2 order, as group n1 = c0.
 template <class PL>
 __device__ __forceinline__ void twist_and_first_ntt(V4* v, uint4* sm, int t, int q, const Tw* tw,
-                                                    const Tw* __restrict__ twist, uint32_t* __restrict__ out_odd,
-                                                    uint64_t ostride, uint64_t col, bool active) {
+                                                    const Tw* __restrict__ twist, const OddOut& oo, uint64_t col,
+                                                    bool active) {
     constexpr int LR = PL::lr(PL::NLEV - 1);
     constexpr int R = 1 << LR;
     constexpr int G = PL::EPT / R;
@@ -227,13 +234,13 @@ __device__ __forceinline__ void twist_and_first_ntt(V4* v, uint4* sm, int t, int
             }
         }
         __syncthreads();
-        ntt_levels<PL, 1>(v, sm, t, q, tw, out_odd, ostride, col, active);
+        ntt_levels<PL, 1>(v, sm, t, q, tw, oo, col, active);
     } else {
         // single level: output index k2 = bitrev(r)
 #pragma unroll
         for (int r = 0; r < R; r++) {
             const uint32_t k = (uint32_t)bitrev(r, LR);
-            if (active) stg_stream_v4(out_odd + (uint64_t)k * ostride + col, v[r]);
+            if (active && k < oo.rows) stg_stream_v4(oo.p + (uint64_t)k * oo.stride + col, v[r]);
         }
     }
 }
@@ -262,7 +269,8 @@ struct TileRange {
 template <int LOG_S, int SCHED = 0, int LEPT = 4>
 __global__ void __launch_bounds__(LEPT == 3 ? 1024 : 512, 1)
     k_extend(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint64_t cols, uint64_t ntiles,
-             const Tw* __restrict__ tw, const Tw* __restrict__ twist_all, uint32_t flags) {
+             const Tw* __restrict__ tw, const Tw* __restrict__ twist_all, uint32_t flags, uint32_t in_rows,
+             uint32_t out_rows) {
     using PL = ExtPlan<LOG_S, SCHED, LEPT, LEPT == 3 ? 1024 : 512>;
     extern __shared__ uint4 sm[];
     const int tid = threadIdx.x;
@@ -270,10 +278,12 @@ __global__ void __launch_bounds__(LEPT == 3 ? 1024 : 512, 1)
     const int t = tid / PL::Q4;
     const Tw* twist = twist_all + PL::S;  // g^i / S for this side, i in [0, S)
     V4 v[PL::EPT];
-    // flags bit 4: write only the odd rows, compactly (out is then [S][cols])
+    // flags bit 4: write only the odd rows, compactly (out is then [S][cols]).
+    // Input rows >= in_rows are zeros (never read); rows >= out_rows of the
+    // interleaved output are not written (an encoding of k < S data rows and
+    // fewer than 2S rows); out_rows = 2S writes everything.
     const bool odd_only = flags & 16;
-    uint32_t* const out_odd = odd_only ? out : out + cols;
-    const uint64_t ostride = odd_only ? cols : 2 * cols;
+    const OddOut oo{odd_only ? out : out + cols, odd_only ? cols : 2 * cols, out_rows / 2};
     const TileRange tr(ntiles, flags & 1);
     for (uint64_t tile = tr.first; tile < tr.last; tile += tr.step) {
         const uint64_t col = tile * PL::C + 4 * (uint64_t)q;
@@ -289,15 +299,12 @@ __global__ void __launch_bounds__(LEPT == 3 ? 1024 : 512, 1)
 #pragma unroll
             for (int j = 0; j < R0; j++) {
                 const uint64_t row = (uint64_t)(g * PL::TPQ + t) + (uint64_t)L0 * j;
-                if (active) {
-                    v[g * R0 + j] = ldg_stream_v4(in + row * cols + col);
-                    if (!odd_only) stg_stream_v4(out + 2 * row * cols + col, v[g * R0 + j]);
-                } else {
-                    v[g * R0 + j] = V4{{0, 0, 0, 0}};
-                }
+                v[g * R0 + j] = active && row < in_rows ? ldg_stream_v4(in + row * cols + col) : V4{{0, 0, 0, 0}};
+                // even rows: the (zero-padded) data
+                if (active && !odd_only && 2 * row < out_rows) stg_stream_v4(out + 2 * row * cols + col, v[g * R0 + j]);
             }
         dif_levels<PL, 0, true>(v, sm, t, q, tw);
-        twist_and_first_ntt<PL>(v, sm, t, q, tw, twist, out_odd, ostride, col, active);
+        twist_and_first_ntt<PL>(v, sm, t, q, tw, twist, oo, col, active);
     }
 }
 

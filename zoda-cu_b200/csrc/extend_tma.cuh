@@ -347,8 +347,7 @@ __device__ __forceinline__ void intt_upto_last(V4* v, uint2* xg, int t, int ql, 
 // the odd output rows.
 template <class TP, int l>
 __device__ __forceinline__ void ntt_from(V4* v, uint2* xg, int t, int ql, int bar, const SideTables& tb,
-                                         uint32_t* __restrict__ out_odd, uint64_t ostride, uint64_t col,
-                                         bool active) {
+                                         const OddOut& oo, uint64_t col, bool active) {
     using LV = LvlGeom<TP, TP::nlr(l), TP::npre(l)>;
     if constexpr (l < TP::NLEV - 1) {
         using Rd = LvlGeom<TP, TP::nlr(l + 1), TP::npre(l + 1)>;
@@ -360,7 +359,7 @@ __device__ __forceinline__ void ntt_from(V4* v, uint2* xg, int t, int ql, int ba
         exchange<TP, LV::R, LV::LOGL, Rd::R, Rd::LOGL>(
             v, xg, ql, bar, [&](int g) { return LV::base(LV::gid(g, t)); },
             [&](int g) { return Rd::base(Rd::gid(g, t)); });
-        ntt_from<TP, l + 1>(v, xg, t, ql, bar, tb, out_odd, ostride, col, active);
+        ntt_from<TP, l + 1>(v, xg, t, ql, bar, tb, oo, col, active);
     } else {
 #pragma unroll
         for (int g = 0; g < LV::G; g++) dft_dif<TP::nlr(l), false>(v + g * LV::R);
@@ -371,7 +370,7 @@ __device__ __forceinline__ void ntt_from(V4* v, uint2* xg, int t, int ql, int ba
             for (int r = 0; r < LV::R; r++) {
                 const uint32_t k =
                     digit_rev<typename TP::PL, true>((blk << TP::nlr(l)) | (uint32_t)bitrev(r, TP::nlr(l)));
-                if (active) stg_stream_v4(out_odd + (uint64_t)k * ostride + col, v[g * LV::R + r]);
+                if (active && k < oo.rows) stg_stream_v4(oo.p + (uint64_t)k * oo.stride + col, v[g * LV::R + r]);
             }
         }
     }
@@ -420,12 +419,12 @@ __device__ __forceinline__ void stage_read(V4* v, const unsigned char* smem, con
 }
 
 // Everything after the tile is in registers: INTT, twist, NTT, odd-row stores
-// (odd row k at out_odd + k * ostride).
+// (see OddOut).
 // With stagger_pending set, group 0 releases group 1 (named barrier 3) when it
 // starts INTT level stagger_at (NLEV-1: after all INTT levels but the last).
 template <class TP>
 __device__ __forceinline__ void tile_compute(V4* v, uint2* xg, const Coords<TP>& c, int bar, const SideTables& tb,
-                                             uint32_t* __restrict__ out_odd, uint64_t ostride, uint64_t col, bool active,
+                                             const OddOut& oo, uint64_t col, bool active,
                                              bool& stagger_pending, int stagger_at = TP::NLEV - 1) {
     const int t = c.t, ql = c.ql;
     // ---- INTT levels 0 .. NLEV-2
@@ -460,7 +459,7 @@ __device__ __forceinline__ void tile_compute(V4* v, uint2* xg, const Coords<TP>&
             [&](int g) { return Rd::base(Rd::gid(g, t)); });
     }
     // ---- NTT levels 1 .. NLEV-1, the last one stores the odd rows
-    ntt_from<TP, 1>(v, xg, t, ql, bar, tb, out_odd, ostride, col, active);
+    ntt_from<TP, 1>(v, xg, t, ql, bar, tb, oo, col, active);
 }
 
 // Re-derive a value from an opaque copy so the compiler rebuilds per-tile
@@ -480,7 +479,7 @@ template <int LOG_S, int LEPT = 4>
 __global__ void __launch_bounds__(TPlan<LOG_S, LEPT>::THREADS, 1)
     k_extend_tma(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_even,
                  uint32_t* __restrict__ out, uint64_t cols, uint64_t ntiles, const SideTables tb,
-                 int* __restrict__ err, uint32_t flags) {
+                 int* __restrict__ err, uint32_t flags, uint32_t out_rows) {
     using TP = TPlan<LOG_S, LEPT>;
     extern __shared__ __align__(1024) unsigned char smem[];
     uint32_t* stage = reinterpret_cast<uint32_t*>(smem);
@@ -500,9 +499,10 @@ __global__ void __launch_bounds__(TPlan<LOG_S, LEPT>::THREADS, 1)
     __syncthreads();
     const TileRange tr(ntiles, flags & 1);
     const bool stagger = !(flags & 2);
-    const bool odd_only = flags & 16;  // only the odd rows, compactly: out is then [S][cols]
-    uint32_t* const out_odd = odd_only ? out : out + cols;
-    const uint64_t ostride = odd_only ? cols : 2 * cols;
+    // bit 4: only the odd rows, compactly (out is then [S][cols]); rows >= out_rows
+    // of the interleaved output are not written (the even-row map is cut there too)
+    const bool odd_only = flags & 16;
+    const OddOut oo{odd_only ? out : out + cols, odd_only ? cols : 2 * cols, out_rows / 2};
     const int stagger_at = (flags >> 2) & 3 ? (int)((flags >> 2) & 3) - 1 : TP::NLEV - 1;
     uint64_t tile = tr.first;
     if (producer && tile < tr.last) tma_load_tile<TP>(stage, &tm_in, tile, full);
@@ -537,7 +537,7 @@ __global__ void __launch_bounds__(TPlan<LOG_S, LEPT>::THREADS, 1)
             if (e_ok) tma_load_tile<TP>(stage, &tm_in, next, full);
             else atomicOr(err, 2);  // both groups then time out on `full` and leave
         }
-        tile_compute<TP>(v, xg, c, bar, tb, out_odd, ostride, col, active, stagger_pending, stagger_at);
+        tile_compute<TP>(v, xg, c, bar, tb, oo, col, active, stagger_pending, stagger_at);
     }
     stagger_release<TP::THREADS>(stagger_pending);
     if (producer) bulk_wait0();
@@ -690,7 +690,8 @@ __global__ void __launch_bounds__(BatchGeom<LEPT>::THREADS, 1)
             else atomicOr(err, 2);                                                               \
         }                                                                                        \
         const uint64_t col = s.tile * TP::C + 4 * (uint64_t)c.q;                                 \
-        tile_compute<TP>(v, xg, c, bar, tb, out + cols, 2 * cols, col, col < cols, stagger_pending); \
+        tile_compute<TP>(v, xg, c, bar, tb, OddOut{out + cols, 2 * cols, (uint32_t)TP::S}, col, col < cols,   \
+                         stagger_pending);                                                       \
     }
         ZB_BATCH_SWITCH(s.log_s, ZB_TILE)
 #undef ZB_TILE

@@ -8,7 +8,9 @@
 // rows 0 .. k+n-1 in natural order. With R = n_kn / n_k, output row R*m + c is
 //   c = 0:  the padded data row m (a copy),
 //   c > 0:  NTT_{n_k}(omega_{n_kn}^(c*i) * coef_i)[m], one transform per coset.
-// Square power-of-two inputs (n = k) go to the fused extension kernels instead.
+// R = 2 (every square, and any n <= 2 n_k - k) runs on the fused extension
+// kernels, which read zeros past row k and stop writing after row k+n; the
+// other shapes take the interpolation + per-coset evaluation path below.
 //
 // Decoder: f of degree < k is known at a set K of the 2k points omega_2k^j.
 // With Z(x) = prod over the erased points of (x - omega^e), g = f * Z has
@@ -261,6 +263,14 @@ zoda_status zoda_encode_device(zoda_ctx* ctx, const uint32_t* d_in, uint32_t* d_
     }
     if (n == k && log2_exact64(k) >= 0) return zoda_extend_device(ctx, d_in, d_out, k, cols, stream);
     if (cols == 0) return ZODA_OK;
+    const uint64_t P_ = next_pow2_64(k), N = next_pow2_64(rows_out);
+    if (N == 2 * P_ && P_ >= 2) {
+        // n_kn = 2 n_k: the fused kernels, reading zeros past row k and cutting
+        // the output after row k+n
+        ZB_CUDA(cudaSetDevice(ctx->device));
+        return launch_extend(ctx, log2_exact64(P_), d_in, d_out, cols, (cudaStream_t)stream, ctx->impl, false, k,
+                             (uint32_t)rows_out);
+    }
     std::lock_guard<std::mutex> lock(ctx->mu);
     ZB_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t st = (cudaStream_t)stream;

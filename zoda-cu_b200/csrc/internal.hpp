@@ -82,15 +82,19 @@ namespace zb {
 // impl: 0 = the side's plan (tuned, or the default), 1 = direct-load kernel,
 // 2 = TMA-staged kernel (sides 32..4096), both with default knobs. With
 // odd_only the kernel writes only the odd rows, as a compact [S][cols] out.
+// in_rows < S: input rows past it are zeros (never read); out_rows < 2S: rows
+// of the interleaved output past it are not written; 0 means S and 2S.
 zoda_status launch_extend(const zoda_ctx* ctx, int log_s, const uint32_t* in, uint32_t* out, uint64_t cols,
-                          cudaStream_t st, int impl = 0, bool odd_only = false);
+                          cudaStream_t st, int impl = 0, bool odd_only = false, uint32_t in_rows = 0,
+                          uint32_t out_rows = 0);
 // The plan a side runs with impl 0 and no tuning.
 zoda_plan default_plan(int log_s);
 // ZODA_OK when the plan can run for this side.
 zoda_status check_plan(int log_s, const zoda_plan& p);
 // Launches one explicit plan.
 zoda_status launch_plan(const zoda_ctx* ctx, int log_s, const zoda_plan& p, const uint32_t* in, uint32_t* out,
-                        uint64_t cols, cudaStream_t st, bool odd_only = false);
+                        uint64_t cols, cudaStream_t st, bool odd_only = false, uint32_t in_rows = 0,
+                        uint32_t out_rows = 0);
 // The L2 promotion a side's TMA loads use on this context (for the batch maps).
 int side_l2_promo(const zoda_ctx* ctx, int log_s);
 // Sets the dynamic shared memory attribute of every extension instantiation.
