@@ -559,7 +559,7 @@ def run_ours(args, world, rank, local):
     ctx = zoda_b200.Context(local)
     side = args.side
     cols = side * SHARE_U32
-    plan = None if args.no_tune else tune(ctx, side, cols)
+    plan = None if args.no_tune else tune(ctx, side, cols, reps=10)
     sampler = ClockSampler(local) if rank == 0 else None
     ms, clocks = time_device_extend(ctx, side, args.steps, args.warmup, world, sampler)
     ms_max = max_over_ranks(ms, world)
@@ -584,7 +584,7 @@ def run_ours(args, world, rank, local):
         for s2 in args.extra_sides:
             if s2 == side:
                 continue
-            plan2 = None if args.no_tune else tune(ctx, s2, s2 * SHARE_U32)
+            plan2 = None if args.no_tune else tune(ctx, s2, s2 * SHARE_U32, reps=3 if s2 >= 4096 else 6)
             ms2, _ = time_device_extend(ctx, s2, max(3, args.steps // 2), 3, 1)
             t2 = ms2 / max(3, args.steps // 2)
             extra[f"side{s2}"] = {

@@ -125,8 +125,9 @@ typedef struct zoda_plan {
  * (cols = 0: about 256 MiB of input, rounded to the side's tile width), with
  * `reps` timed runs after one warm-up. A candidate whose output differs in
  * any bit from the default plan's is rejected. The fastest is installed on
- * the context and written to plans[log2(side)] when `plans` is not NULL
- * (an array of 13). Allocates and frees its own buffers; synchronous. */
+ * the context (the default plan instead when it is within 1% of the fastest)
+ * and written to plans[log2(side)] when `plans` is not NULL (an array of 13).
+ * Allocates and frees its own buffers; synchronous. */
 zoda_status zoda_autotune(zoda_ctx* ctx, uint32_t side_min, uint32_t side_max, uint64_t cols, uint32_t reps,
                           zoda_plan* plans);
 /* Reads (ZODA_ERR_STATE when the side has no plan) or installs the plan of

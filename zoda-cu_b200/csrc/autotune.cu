@@ -6,7 +6,8 @@
 // candidate once, counts the words that differ from the reference on the
 // device (a candidate with any difference is rejected), and times `reps`
 // back-to-back launches with CUDA events on the context's stream. The
-// fastest survivor becomes the side's plan on the context.
+// fastest survivor becomes the side's plan on the context, unless the default
+// plan is within 1% of it (then the default stays).
 //
 // Candidates: the direct-load kernel with radix-16 or radix-8 levels (512 or
 // 1024 threads), either radix schedule and either tile order; the TMA-staged kernel (sides >= 32) with radix-16 or radix-8
@@ -136,6 +137,7 @@ zoda_status tune_side(zoda_ctx* ctx, int ls, uint64_t cols, uint32_t reps, zoda_
     zoda_plan best{};
     float best_ms = 0.f;
     bool have = false;
+    float default_ms = -1.f;  // cand[0] is the default plan
     for (const zoda_plan& p : cand) {
         ZB_CUDA(cudaMemsetAsync(b.out, 0xFF, nout * 4, st));
         if ((s = launch_plan(ctx, ls, p, in, (uint32_t*)b.out, cols, st)) != ZODA_OK) return s;
@@ -155,6 +157,7 @@ zoda_status tune_side(zoda_ctx* ctx, int ls, uint64_t cols, uint32_t reps, zoda_
         float ms = 0.f;
         ZB_CUDA(cudaEventElapsedTime(&ms, b.e0, b.e1));
         ms /= (float)reps;
+        if (&p == &cand[0]) default_ms = ms;
         if (!have || ms < best_ms) {
             best = p;
             best_ms = ms;
@@ -164,6 +167,12 @@ zoda_status tune_side(zoda_ctx* ctx, int ls, uint64_t cols, uint32_t reps, zoda_
     if (!have) {
         set_last_error_text("autotune: no candidate reproduced the default plan's output");
         return ZODA_ERR_STATE;
+    }
+    // Keep the default unless a candidate beats it by more than 1%: nearer
+    // than that, the difference is within run-to-run noise.
+    if (default_ms >= 0.f && default_ms <= best_ms * 1.01f) {
+        best = cand[0];
+        best_ms = default_ms;
     }
     best.ms = best_ms;
     *best_out = best;
