@@ -30,10 +30,11 @@ struct ColTx {
     uint64_t cols;  // multiple of 4
 };
 
-template <int LOG_N, bool INV>
-__global__ void __launch_bounds__(512, 1)
+// LEPT 4: radix-16 levels, 512 threads; 3: radix-8 levels, 1024 threads.
+template <int LOG_N, bool INV, int LEPT = 4>
+__global__ void __launch_bounds__(LEPT == 3 ? 1024 : 512, 1)
     k_coltx(const ColTx a, uint64_t ntiles, const Tw* __restrict__ tw) {
-    using PL = ExtPlan<LOG_N>;
+    using PL = ExtPlan<LOG_N, 0, LEPT, LEPT == 3 ? 1024 : 512>;
     extern __shared__ uint4 sm[];
     const int tid = threadIdx.x;
     const int q = tid % PL::Q4;
