@@ -570,17 +570,20 @@ def run_ours(args, world, rank, local):
     achieved = alg_bytes / (ms / args.steps * 1e-3) / 1e9
     traffic = ncu_traffic(f"k_extend_side{side}")
     extra = {}
-    e2e = None
     cpu = None
-    if rank == 0:
-        e2e_ms, parts, h2d, d2h = time_host_extend(ctx, side, max(2, min(args.steps, 5)), 1)
-        e2e = {"value": round(payload_bits(side) / (e2e_ms * 1e-3) / 1e9, 3), "unit": "Gb/s",
-               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_ms, 3),
-               "split_ms": parts,
-               "api": "zoda_extend_host (pinned host buffers; odd rows over PCIe, even rows copied on the host)"}
+    # e2e: every rank encodes its own square from host buffers at the same time; the slowest sets the step
+    barrier(world)
+    e2e_ms, parts, h2d, d2h = time_host_extend(ctx, side, max(2, min(args.steps, 5)), 1)
+    e2e_max = max_over_ranks(e2e_ms, world)
+    e2e = {"value": round(job_rate(world, side, e2e_max, 1), 3), "unit": "Gb/s",
+           "h2d_bytes_per_step": world * h2d, "d2h_bytes_per_step": world * d2h, "ms_per_step": round(e2e_max, 3),
+           "split_ms": parts,
+           "api": "zoda_extend_host (pinned host buffers; odd rows over PCIe, even rows copied on the host)"}
     if world > 1:
         barrier(world)
-    if rank == 0 and not args.no_extra:
+    # report-only extras and the CPU baseline: rank 0 of a 1-GPU run only (they would hold the other
+    # ranks at the next barrier for a minute or more)
+    if rank == 0 and world == 1 and not args.no_extra:
         for s2 in args.extra_sides:
             if s2 == side:
                 continue
@@ -604,7 +607,7 @@ def run_ours(args, world, rank, local):
             # where launch overhead dominates: the same draw restricted to sides 32..256
             extra["batched_small_squares"] = time_batched(ctx, args.batch_squares, hi=256)
             extra["serving"] = time_serving(ctx, args.serve_rate, args.serve_requests)
-    if rank == 0:
+    if rank == 0 and world == 1:
         cpu = cpu_port_rate(side, args.cpu_budget)
         cpu.pop("seconds", None)
     if world > 1:
