@@ -68,6 +68,65 @@ def test_rlc_rows_extreme_values(ctx):
     assert np.array_equal(from_dev(out).astype(np.uint64), O.rlc_rows(m, coeff))
 
 
+def test_rlc_rows_any_u32(ctx):
+    """Row values and coefficients over the whole u32 range (p, 2p, 2^32 - 1 among
+    them): the sums are those of the values' residues."""
+    rows, cols = 13, 8200
+    rng = np.random.default_rng(17)
+    m = rng.integers(0, 1 << 32, size=(rows, cols), dtype=np.uint64)
+    m[0, :6] = [P, 2 * P, 2 * P - 1, (1 << 32) - 1, P - 1, 0]
+    m[1] = (1 << 32) - 1
+    coeff = rng.integers(0, 1 << 32, size=(cols, 4), dtype=np.uint64)
+    out = torch.empty((rows, 4), dtype=torch.int32, device="cuda")
+    ctx.rlc_rows(to_dev(m.astype(np.uint32)), rows, cols, to_dev(coeff.astype(np.uint32)), out)
+    torch.cuda.synchronize()
+    assert np.array_equal(from_dev(out).astype(np.uint64), O.rlc_rows(m, coeff))
+
+
+def test_rlc_rows_wide_and_short(ctx):
+    rows, cols = 3, 1 << 20
+    m = O.seeded_input(rows, cols, seed=23)
+    coeff = np.random.default_rng(29).integers(0, P, size=(cols, 4), dtype=np.uint64)
+    out = torch.empty((rows, 4), dtype=torch.int32, device="cuda")
+    ctx.rlc_rows(to_dev(m), rows, cols, to_dev(coeff.astype(np.uint32)), out)
+    torch.cuda.synchronize()
+    assert np.array_equal(from_dev(out).astype(np.uint64), O.rlc_rows(m, coeff))
+
+
+HALF = (P - 1) // 2
+
+
+@pytest.mark.parametrize("xv,cv", [(P - 1, P - 1), (HALF + 1, HALF + 1), (HALF, HALF + 1), (HALF, HALF),
+                                   ((1 << 32) - 1, HALF + 1)])
+def test_rlc_rows_full_size_worst_case(ctx, xv, cv):
+    """The 1024 square's 2048 x 131072 code matrix with one value everywhere and
+    one coefficient in every limb: residues at +-(p-1)/2 give the largest product
+    magnitudes of either sign (p - 1 the largest canonical value), so every
+    partial sum runs at its bound. Every limb is cols * x * c mod p."""
+    rows, cols = 2048, 131072
+    to_i32 = lambda v: v - (1 << 32) if v >= 1 << 31 else v
+    x = torch.full((rows, cols), to_i32(xv), dtype=torch.int32, device="cuda")
+    coeff = torch.full((cols, 4), to_i32(cv), dtype=torch.int32, device="cuda")
+    out = torch.empty((rows, 4), dtype=torch.int32, device="cuda")
+    ctx.rlc_rows(x, rows, cols, coeff, out)
+    torch.cuda.synchronize()
+    assert bool((out == cols * (xv % P) * cv % P).all())
+
+
+def test_rlc_rows_full_size_sampled(ctx):
+    """Random 2048 x 131072 matrix: sampled rows against the oracle."""
+    rows, cols = 2048, 131072
+    gen = torch.Generator(device="cuda").manual_seed(31)
+    x = torch.randint(0, P, (rows, cols), dtype=torch.int64, device="cuda", generator=gen).to(torch.int32)
+    coeff = torch.randint(0, P, (cols, 4), dtype=torch.int64, device="cuda", generator=gen).to(torch.int32)
+    out = torch.empty((rows, 4), dtype=torch.int32, device="cuda")
+    ctx.rlc_rows(x, rows, cols, coeff, out)
+    torch.cuda.synchronize()
+    pick = [0, 1, 3, 4, 5, 1023, 1024, 2046, 2047] + list(np.random.default_rng(37).integers(0, rows, 7))
+    want = O.rlc_rows(from_dev(x[pick]).astype(np.uint64), from_dev(coeff).astype(np.uint64))
+    assert np.array_equal(from_dev(out)[pick].astype(np.uint64), want)
+
+
 def reference_flow(ctx, data, n):
     """encode -> data root (host) -> coefficients (device) -> RLC check of every row."""
     import zoda_b200

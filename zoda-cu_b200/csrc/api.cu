@@ -241,6 +241,7 @@ zoda_status zoda_ctx_create(int device, zoda_ctx** out) {
         }
     }
     zoda_status s = extend_init_attributes();
+    if (s == ZODA_OK) s = rlc_init_attributes();
     if (s != ZODA_OK) return fail(s);
     *out = c;
     return ZODA_OK;

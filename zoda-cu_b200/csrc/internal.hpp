@@ -71,9 +71,9 @@ struct zoda_ctx {
     zb::DevBuf gen_a, gen_b, gen_tab, gen_small;
     std::map<int, zb::DevBuf> coset_tabs;
     cudaEvent_t gen_done = nullptr;
-    // RLC consumers (rlc.cu): coefficient tables with Shoup companions, row
+    // RLC consumers (rlc.cu): canonical coefficient table, row
     // accumulators and the check's matrices, under their own lock
-    zb::DevBuf rlc_w, rlc_ws, rlc_acc, rlc_d, rlc_e, rlc_f, rlc_cnt;
+    zb::DevBuf rlc_w, rlc_acc, rlc_d, rlc_e, rlc_f, rlc_cnt;
     std::mutex rlc_mu;
 };
 
@@ -101,6 +101,8 @@ int side_l2_promo(const zoda_ctx* ctx, int log_s);
 zoda_status extend_init_attributes();
 // Frees what the general encode / decoder left in the context.
 void general_release(zoda_ctx* ctx);
+// Sets the dynamic shared memory attribute of the RLC row kernel.
+zoda_status rlc_init_attributes();
 // Frees the RLC consumers' scratch.
 void rlc_release(zoda_ctx* ctx);
 }  // namespace zb

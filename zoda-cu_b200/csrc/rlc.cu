@@ -10,17 +10,20 @@
 //                  root's whole 64-byte blocks compressed once on the host.
 //   rows           rlc[r][l] = sum_c x[r][c] * coeff[c][l] mod p
 //                  (src/zoda/rlc.rs:32-40) as a device reduction over the
-//                  row-major matrix: one HBM read of it, Shoup products with
-//                  the coefficients' companions, 64-bit lazy sums.
+//                  row-major matrix: one HBM read of it through a bulk-copy
+//                  ring, centered residues, signed 64-bit sums of wide
+//                  products with one shift-and-add fold per eight.
 //   check          RLC(encoded row j) == extension of the data rows' RLC at j,
 //                  limb for limb, for EVERY row (the reference samples 64:
 //                  utils.rs:225-272); the extension of the k x 4 RLC matrix is
 //                  the library's own encode with cols = 4.
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
 #include "internal.hpp"
+#include "async.cuh"
 #include "sha256.hpp"
 
 namespace zb {
@@ -151,77 +154,233 @@ __global__ void k_rlc_coeff(const CoeffJob job, uint64_t ncols, uint32_t* __rest
     }
 }
 
-// Shoup companions of the coefficient limbs, one uint4 pair per column.
-__global__ void k_rlc_prep(const uint4* __restrict__ coeff, uint64_t ncols, uint4* __restrict__ w,
-                           uint4* __restrict__ ws) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < ncols;
+// ---- per-row RLC --------------------------------------------------------------
+// Residues are handled in centered form, r - p for r > (p-1)/2, so |x|, |c| <=
+// (p-1)/2 and a product is below 2^60 in magnitude: eight of them on top of a
+// folded sum stay inside a signed 64-bit word (0.95 * 2^63 at worst), and a
+// product is one signed wide multiply-add. 2^32 = 2p + (2^28 - 2) gives the
+// fold h*2^32 + lo == h*(2^28 - 2) + lo (mod p), done with shifts and adds so
+// that the multiply pipe only carries the products; its result lies in
+// (-2^59, 2^59 + 2^32).
+constexpr uint32_t HALF_P = (P - 1) / 2;
+constexpr uint32_t TWO32_MOD_P = 268435454u;
+static_assert((uint64_t)TWO32_MOD_P == (1ull << 32) - 2ull * P && TWO32_MOD_P == (1u << 28) - 2, "2^32 mod p");
+// p * 2^29 exceeds every folded magnitude: adding it makes a folded sum a
+// non-negative value below 2^62 with the same residue.
+constexpr uint64_t P_SHIFT29 = (uint64_t)P << 29;
+
+__host__ __device__ __forceinline__ int32_t centered(uint32_t r) {  // r in [0, p)
+    return (int32_t)(r > HALF_P ? r - P : r);
+}
+__device__ __forceinline__ int64_t sfold(int64_t a) {
+    const int64_t h = a >> 32;  // floor(a / 2^32)
+    return (h << 28) - (h << 1) + (int64_t)(uint32_t)a;
+}
+// unsigned fold for the final reduction: a < 2^64 -> a' == a (mod p), a' < 2^60
+__device__ __forceinline__ uint64_t fold32(uint64_t a) {
+    return (uint64_t)(uint32_t)(a >> 32) * TWO32_MOD_P + (uint32_t)a;
+}
+
+// Centered copy of the coefficient limbs (a caller's table may hold any u32)
+// in four planes: plane j holds, for every column quad q, the four limbs of
+// column 4q + j, so one plane of a column chunk is one contiguous copy.
+__global__ void k_rlc_prep(const uint4* __restrict__ coeff, uint64_t quads, int4* __restrict__ w) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < 4 * quads;
          i += (uint64_t)gridDim.x * blockDim.x) {
-        uint4 c = coeff[i];
-        c.x %= P;  // canonical limbs (a caller's table may hold any u32)
-        c.y %= P;
-        c.z %= P;
-        c.w %= P;
-        w[i] = c;
-        ws[i] = make_uint4(shoup(c.x), shoup(c.y), shoup(c.z), shoup(c.w));
+        const uint4 c = coeff[i];
+        w[(i & 3) * quads + (i >> 2)] =
+            make_int4(centered(c.x % P), centered(c.y % P), centered(c.z % P), centered(c.w % P));
     }
 }
 
-// 4 rows per CTA: 16 lazy 64-bit sums per thread keep the kernel at two
-// 256-thread CTAs per SM (measured 1.5x faster than 8 rows at one CTA).
-constexpr int RB = 4;  // rows per CTA
+__device__ __forceinline__ int32_t limb(const int4& v, int l) {
+    return l == 0 ? v.x : l == 1 ? v.y : l == 2 ? v.z : v.w;
+}
 
-// acc[r][l] += (sum over this CTA's columns of x[r][c] * coeff[c][l]) mod p
-__global__ void __launch_bounds__(256, 2) k_rlc_rows(const uint32_t* __restrict__ x, uint64_t pitch,
-                                                               uint32_t rows, uint64_t quads,
-                                                               const uint4* __restrict__ cw,
-                                                               const uint4* __restrict__ cws,
-                                                               unsigned long long* __restrict__ acc) {
-    const uint32_t r0 = blockIdx.y * RB;
-    uint64_t s[RB][4];
+// Warp sum of NV values per lane (NV = 16 or 32) that halves the set at each
+// exchange: at offset o a lane keeps one half, sends the other and adds what
+// its partner sent for the kept half. NV - 1 64-bit shuffles (plus one for
+// NV = 16) instead of 5 * NV. Afterwards v[0] holds the warp's total of value
+// lane >> 1 (NV = 16) or lane (NV = 32).
+template <int NV>
+__device__ __forceinline__ void warp_sum_split(uint64_t (&v)[NV], int lane) {
 #pragma unroll
-    for (int r = 0; r < RB; r++)
+    for (int h = NV / 2; h >= 1; h >>= 1) {
+        const int o = h * 32 / NV;
+        const bool up = lane & o;
 #pragma unroll
-        for (int l = 0; l < 4; l++) s[r][l] = 0;
-    for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < quads; q += (uint64_t)gridDim.x * blockDim.x) {
-        uint4 w[4], ws[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            w[j] = __ldg(cw + 4 * q + j);
-            ws[j] = __ldg(cws + 4 * q + j);
-        }
-#pragma unroll
-        for (int r = 0; r < RB; r++) {
-            if (r0 + r >= rows) break;
-            const uint4 v = __ldcs(reinterpret_cast<const uint4*>(x + (uint64_t)(r0 + r) * pitch) + q);
-            const uint32_t xv[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                s[r][0] += mul_lazy(xv[j], w[j].x, ws[j].x);
-                s[r][1] += mul_lazy(xv[j], w[j].y, ws[j].y);
-                s[r][2] += mul_lazy(xv[j], w[j].z, ws[j].z);
-                s[r][3] += mul_lazy(xv[j], w[j].w, ws[j].w);
-            }
+        for (int i = 0; i < h; i++) {
+            const uint64_t send = up ? v[i] : v[i + h];
+            const uint64_t keep = up ? v[i + h] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xFFFFFFFFu, send, o);
         }
     }
-    __shared__ unsigned long long red[8][RB * 4];
-    static_assert(RB * 4 <= 256, "one thread per (row, limb) in the final step");
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-    for (int r = 0; r < RB; r++)
-#pragma unroll
-        for (int l = 0; l < 4; l++) {
-            uint64_t v = s[r][l] % P;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
-            if (lane == 0) red[wid][r * 4 + l] = v;
+    if (NV == 16) v[0] += __shfl_xor_sync(0xFFFFFFFFu, v[0], 1);
+}
+
+// The work is the sequence of units (row block rb, column chunk ch), row block
+// major: u = rb * nch + ch. CTA b of G takes units [b*U/G, (b+1)*U/G), so every
+// CTA gets the same share to one unit. A unit is UROWS rows x CHQ column quads
+// of the matrix plus the chunk's four coefficient planes; the producer warp
+// brings it into one of NST shared-memory stages with 1D bulk copies, one copy
+// per lane, and CG groups of 256 consumer threads (RPT rows each, QPU quads per
+// thread) fold it into their sums. The sums are flushed (reduced, then added to
+// acc) when the row block changes and at the end of the range.
+namespace rlcb {
+constexpr int CG = 2;
+constexpr int RPT = 4;
+constexpr int UROWS = CG * RPT;
+constexpr int QPU = 2;  // quads per consumer thread per unit: 4 * QPU <= 8 products per fold
+constexpr int CHQ = 256 * QPU;
+constexpr int NST = 2;
+constexpr int X_BYTES = UROWS * CHQ * 16;
+constexpr int STAGE_BYTES = X_BYTES + 4 * CHQ * 16;
+constexpr int OFF_RED = NST * STAGE_BYTES;
+constexpr int NV = RPT * 4;
+constexpr int OFF_BAR = OFF_RED + CG * 8 * NV * 8;
+constexpr int SMEM = OFF_BAR + 2 * NST * 8;
+constexpr int THREADS = CG * 256 + 32;
+static_assert(QPU >= 1 && QPU <= 2, "at most eight centered products between folds");
+static_assert(NV == 16 || NV == 32, "warp_sum_split takes 16 or 32 values");
+static_assert(SMEM <= 227 * 1024, "shared memory per CTA");
+static_assert(UROWS + 4 <= 32, "one producer lane per copy");
+}  // namespace rlcb
+
+// acc[r][l] += (sum over the CTA's columns of x[r][c] * coeff[c][l]) mod p;
+// x may hold any u32 (reduced on load), cw is the centered planar table.
+__global__ void __launch_bounds__(rlcb::THREADS, 1) k_rlc_rows(const uint32_t* __restrict__ x, uint64_t pitch,
+                                                               uint32_t rows, uint64_t quads,
+                                                               const int4* __restrict__ cw,
+                                                               unsigned long long* __restrict__ acc,
+                                                               int* __restrict__ err) {
+    using namespace rlcb;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + OFF_BAR);  // stage landed (bulk tx)
+    uint64_t* empty = full + NST;                                   // every consumer warp is done with it
+    const int tid = threadIdx.x;
+    const uint64_t nch = (quads + CHQ - 1) / CHQ;
+    const uint64_t U = nch * ((rows + UROWS - 1) / UROWS);
+    const uint64_t u0 = U * blockIdx.x / gridDim.x, u1 = U * (blockIdx.x + 1) / gridDim.x;
+    if (tid == 0) {
+        for (int s = 0; s < NST; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], CG * 8);
         }
+        fence_mbar_init();
+    }
     __syncthreads();
-    if (threadIdx.x < RB * 4) {
-        const int r = threadIdx.x / 4;
-        if (r0 + r < rows) {
-            uint64_t v = 0;
-            for (int w2 = 0; w2 < (int)(blockDim.x / 32); w2++) v += red[w2][threadIdx.x];
-            atomicAdd(acc + (uint64_t)(r0 + r) * 4 + (threadIdx.x & 3), (unsigned long long)(v % P));
+    // the unit's position is carried along (no division per unit): row block rb,
+    // chunk ch, stage s and that stage's phase parity ph
+    const uint32_t rb0 = (uint32_t)(u0 / nch);
+    const uint64_t ch0 = u0 % nch;
+    if (tid >= CG * 256) {  // producer warp
+        const int pl = tid - CG * 256;
+        uint32_t rb = rb0, ph = 0;
+        uint64_t ch = ch0;
+        int s = 0;
+        bool reuse = false;  // from the second pass over the stages on
+        for (uint64_t u = u0; u < u1; u++) {
+            if (reuse) {
+                bool ok = true;
+                if (pl == 0) ok = mbar_wait_bounded(&empty[s], ph ^ 1);
+                if (!__shfl_sync(0xFFFFFFFFu, ok, 0)) {
+                    if (pl == 0) atomicOr(err, 4);  // the consumers then time out on `full` and leave
+                    return;
+                }
+                fence_proxy_async();
+            }
+            const uint32_t r0 = rb * UROWS;
+            const uint64_t q0 = ch * CHQ;
+            const uint32_t bytes = (uint32_t)min((uint64_t)CHQ, quads - q0) * 16;
+            const uint32_t nr = min((uint32_t)UROWS, rows - r0);
+            unsigned char* st = smem + s * STAGE_BYTES;
+            if (pl == 0) mbar_expect_tx(&full[s], bytes * (nr + 4));
+            __syncwarp();
+            if (pl < (int)nr)
+                bulk_load_1d(st + pl * CHQ * 16, x + (uint64_t)(r0 + pl) * pitch + q0 * 4, bytes, &full[s]);
+            else if (pl >= UROWS && pl < UROWS + 4)
+                bulk_load_1d(st + X_BYTES + (pl - UROWS) * CHQ * 16, cw + (pl - UROWS) * quads + q0, bytes, &full[s]);
+            if (++s == NST) {
+                s = 0;
+                ph ^= 1;
+                reuse = true;
+            }
+            if (++ch == nch) {
+                ch = 0;
+                rb++;
+            }
+        }
+        return;
+    }
+    const int g = tid >> 8, t = tid & 255, lane = tid & 31;
+    const int bar = 1 + g;
+    int64_t sum[NV];
+#pragma unroll
+    for (int i = 0; i < NV; i++) sum[i] = 0;
+    unsigned long long* red = reinterpret_cast<unsigned long long*>(smem + OFF_RED) + g * 8 * NV;
+    uint32_t rb = rb0, ph = 0;
+    uint64_t ch = ch0;
+    int s = 0;
+    for (uint64_t u = u0; u < u1; u++) {
+        const bool ok = mbar_wait_bounded(&full[s], ph);
+        if (group_vote_or(bar, !ok, 256)) {
+            if (t == 0) atomicOr(err, 1);
+            return;
+        }
+        const uint32_t rg = rb * UROWS + g * RPT;  // this group's first row
+        const uint64_t qb = ch * CHQ;
+        const uint4* sx = reinterpret_cast<const uint4*>(smem + s * STAGE_BYTES);
+        const int4* sc = reinterpret_cast<const int4*>(smem + s * STAGE_BYTES + X_BYTES);
+#pragma unroll
+        for (int k = 0; k < QPU; k++) {
+            const int qi = k * 256 + t;
+            if (qb + qi >= quads) break;
+            int4 w[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) w[j] = sc[j * CHQ + qi];
+#pragma unroll
+            for (int r = 0; r < RPT; r++) {
+                if (rg + r >= rows) break;
+                const uint4 v = sx[(g * RPT + r) * CHQ + qi];
+                const int32_t xv[4] = {centered(reduce_2p(reduce_2p(v.x))), centered(reduce_2p(reduce_2p(v.y))),
+                                       centered(reduce_2p(reduce_2p(v.z))), centered(reduce_2p(reduce_2p(v.w)))};
+#pragma unroll
+                for (int l = 0; l < 4; l++)
+#pragma unroll
+                    for (int j = 0; j < 4; j++) sum[r * 4 + l] += (int64_t)xv[j] * limb(w[j], l);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < NV; k++) sum[k] = sfold(sum[k]);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
+        if (u + 1 == u1 || ch + 1 == nch) {
+            // flush: + p*2^29 makes the folded sums non-negative below 2^62, one fold
+            // brings them below 2^57 (32 lanes < 2^62), the warp totals fold again
+            // (8 warps < 2^62)
+            uint64_t v[NV];
+#pragma unroll
+            for (int k = 0; k < NV; k++) v[k] = fold32((uint64_t)(sum[k] + (int64_t)P_SHIFT29));
+            warp_sum_split<NV>(v, lane);
+            if (NV == 32 || !(lane & 1)) red[(t >> 5) * NV + (NV == 32 ? lane : lane >> 1)] = fold32(v[0]);
+            group_bar(bar, 256);
+            if (t < NV && rg + t / 4 < rows) {
+                uint64_t r = 0;
+#pragma unroll
+                for (int w2 = 0; w2 < 8; w2++) r += red[w2 * NV + t];
+                atomicAdd(acc + (uint64_t)(rg + t / 4) * 4 + (t & 3), (unsigned long long)(r % P));
+            }
+            group_bar(bar, 256);  // red is free for the next flush
+#pragma unroll
+            for (int k = 0; k < NV; k++) sum[k] = 0;
+        }
+        if (++s == NST) {
+            s = 0;
+            ph ^= 1;
+        }
+        if (++ch == nch) {
+            ch = 0;
+            rb++;
         }
     }
 }
@@ -246,20 +405,19 @@ unsigned grid1(const zoda_ctx* ctx, uint64_t n) {
     return (unsigned)(g < 1 ? 1 : g > cap ? cap : g);
 }
 
-// rlc of rows [rows][cols] (pitch cols) into out [rows][4]; tables w/ws prepared.
-zoda_status rlc_rows(const zoda_ctx* ctx, const uint32_t* x, uint32_t rows, uint64_t cols, const uint4* w,
-                     const uint4* ws, unsigned long long* acc, uint32_t* out, cudaStream_t st) {
+// rlc of rows [rows][cols] (pitch cols) into out [rows][4]; table w prepared.
+zoda_status rlc_rows(const zoda_ctx* ctx, const uint32_t* x, uint32_t rows, uint64_t cols, const int4* w,
+                     unsigned long long* acc, uint32_t* out, cudaStream_t st) {
     ZB_CUDA(cudaMemsetAsync(acc, 0, (size_t)rows * 4 * sizeof(unsigned long long), st));
     const uint64_t quads = cols / 4;
-    const uint32_t gy = (rows + RB - 1) / RB;
-    uint64_t gx = (quads + 256 * 8 - 1) / (256 * 8) * (8 / RB);  // ~RB column quads per thread
-    if (gx < 1) gx = 1;
-    if (gy > 65535) {
+    if (rows > 262140) {
         set_last_error_text("rlc: more than 262140 rows");
         return ZODA_ERR_UNSUPPORTED;
     }
     if (quads) {
-        k_rlc_rows<<<dim3((unsigned)gx, gy), 256, 0, st>>>(x, cols, rows, quads, w, ws, acc);
+        const uint64_t units = (quads + rlcb::CHQ - 1) / rlcb::CHQ * ((rows + rlcb::UROWS - 1) / rlcb::UROWS);
+        const unsigned g = (unsigned)std::min<uint64_t>(units, (uint64_t)ctx->sm_count);
+        k_rlc_rows<<<g, rlcb::THREADS, rlcb::SMEM, st>>>(x, cols, rows, quads, w, acc, ctx->d_err);
         ZB_CUDA(cudaGetLastError());
     }
     k_rlc_final<<<grid1(ctx, (uint64_t)rows * 4), 256, 0, st>>>(acc, (uint64_t)rows * 4, out);
@@ -270,17 +428,20 @@ zoda_status rlc_rows(const zoda_ctx* ctx, const uint32_t* x, uint32_t rows, uint
 zoda_status prep_tables(zoda_ctx* ctx, const uint32_t* d_coeff, uint64_t cols, cudaStream_t st) {
     zoda_status s;
     if ((s = ctx->rlc_w.ensure(cols * 16 + 16)) != ZODA_OK) return s;
-    if ((s = ctx->rlc_ws.ensure(cols * 16 + 16)) != ZODA_OK) return s;
-    k_rlc_prep<<<grid1(ctx, cols), 256, 0, st>>>((const uint4*)d_coeff, cols, (uint4*)ctx->rlc_w.p,
-                                                 (uint4*)ctx->rlc_ws.p);
+    k_rlc_prep<<<grid1(ctx, cols), 256, 0, st>>>((const uint4*)d_coeff, cols / 4, (int4*)ctx->rlc_w.p);
     ZB_CUDA(cudaGetLastError());
     return ZODA_OK;
 }
 
 }  // namespace
 
+zoda_status rlc_init_attributes() {
+    ZB_CUDA(cudaFuncSetAttribute(k_rlc_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, rlcb::SMEM));
+    return ZODA_OK;
+}
+
 void rlc_release(zoda_ctx* ctx) {
-    for (DevBuf* b : {&ctx->rlc_w, &ctx->rlc_ws, &ctx->rlc_acc, &ctx->rlc_d, &ctx->rlc_e, &ctx->rlc_f, &ctx->rlc_cnt})
+    for (DevBuf* b : {&ctx->rlc_w, &ctx->rlc_acc, &ctx->rlc_d, &ctx->rlc_e, &ctx->rlc_f, &ctx->rlc_cnt})
         b->release();
 }
 
@@ -347,7 +508,7 @@ zoda_status zoda_rlc_rows_device(zoda_ctx* ctx, const uint32_t* d_rows, uint32_t
     zoda_status s = prep_tables(ctx, d_coeff, cols, st);
     if (s != ZODA_OK) return s;
     if ((s = ctx->rlc_acc.ensure((size_t)rows * 4 * 8)) != ZODA_OK) return s;
-    return rlc_rows(ctx, d_rows, rows, cols, (const uint4*)ctx->rlc_w.p, (const uint4*)ctx->rlc_ws.p,
+    return rlc_rows(ctx, d_rows, rows, cols, (const int4*)ctx->rlc_w.p,
                     (unsigned long long*)ctx->rlc_acc.p, d_out, st);
 }
 
@@ -367,14 +528,13 @@ zoda_status zoda_rlc_check_device(zoda_ctx* ctx, const uint32_t* d_data, const u
     if ((s = ctx->rlc_e.ensure((size_t)rows * 16)) != ZODA_OK) return s;
     if ((s = ctx->rlc_f.ensure((size_t)rows * 16)) != ZODA_OK) return s;
     if ((s = ctx->rlc_cnt.ensure(8)) != ZODA_OK) return s;
-    const uint4* w = (const uint4*)ctx->rlc_w.p;
-    const uint4* ws = (const uint4*)ctx->rlc_ws.p;
+    const int4* w = (const int4*)ctx->rlc_w.p;
     unsigned long long* acc = (unsigned long long*)ctx->rlc_acc.p;
     uint32_t *D = (uint32_t*)ctx->rlc_d.p, *E = (uint32_t*)ctx->rlc_e.p, *F = (uint32_t*)ctx->rlc_f.p;
-    if ((s = rlc_rows(ctx, d_data, k, cols, w, ws, acc, D, st)) != ZODA_OK) return s;
+    if ((s = rlc_rows(ctx, d_data, k, cols, w, acc, D, st)) != ZODA_OK) return s;
     // the RLC and the extension commute (both F_p-linear): extend the k x 4 RLC matrix
     if ((s = zoda_encode_device(ctx, D, F, k, n, 4, st)) != ZODA_OK) return s;
-    if ((s = rlc_rows(ctx, d_code, rows, cols, w, ws, acc, E, st)) != ZODA_OK) return s;
+    if ((s = rlc_rows(ctx, d_code, rows, cols, w, acc, E, st)) != ZODA_OK) return s;
     ZB_CUDA(cudaMemsetAsync(ctx->rlc_cnt.p, 0, 8, st));
     k_count_diff<<<grid1(ctx, (uint64_t)rows * 4), 256, 0, st>>>(E, F, (uint64_t)rows * 4,
                                                                 (unsigned long long*)ctx->rlc_cnt.p);
