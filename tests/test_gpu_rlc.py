@@ -47,7 +47,10 @@ def test_coefficients_of_a_data_root(ctx):
     assert np.array_equal(from_dev(d).astype(np.uint64), O.coefficients(root, 8192))
 
 
-@pytest.mark.parametrize("rows,cols", [(1, 4), (37, 4100), (8, 131072), (300, 512)])
+# shapes on both kernels: a thread per column quad below 256 rows, a thread per
+# row from 256 on (ragged row blocks of 512, ragged and narrow 32-column chunks)
+@pytest.mark.parametrize("rows,cols", [(1, 4), (37, 4100), (8, 131072), (255, 1028), (256, 4), (300, 512),
+                                       (300, 36), (513, 4100), (1000, 20), (1536, 8192)])
 def test_rlc_rows_match_oracle(ctx, rows, cols):
     m = O.seeded_input(rows, cols, seed=rows + cols)
     rng = np.random.default_rng(3)
@@ -68,10 +71,11 @@ def test_rlc_rows_extreme_values(ctx):
     assert np.array_equal(from_dev(out).astype(np.uint64), O.rlc_rows(m, coeff))
 
 
-def test_rlc_rows_any_u32(ctx):
+@pytest.mark.parametrize("rows", [13, 300])
+def test_rlc_rows_any_u32(ctx, rows):
     """Row values and coefficients over the whole u32 range (p, 2p, 2^32 - 1 among
     them): the sums are those of the values' residues."""
-    rows, cols = 13, 8200
+    cols = 8200
     rng = np.random.default_rng(17)
     m = rng.integers(0, 1 << 32, size=(rows, cols), dtype=np.uint64)
     m[0, :6] = [P, 2 * P, 2 * P - 1, (1 << 32) - 1, P - 1, 0]

@@ -17,14 +17,15 @@
 //                  limb for limb, for EVERY row (the reference samples 64:
 //                  utils.rs:225-272); the extension of the k x 4 RLC matrix is
 //                  the library's own encode with cols = 4.
-#include <cstdio>
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <vector>
 
-#include "internal.hpp"
 #include "async.cuh"
+#include "internal.hpp"
 #include "sha256.hpp"
+#include "tma_host.hpp"
 
 namespace zb {
 namespace sha {
@@ -169,9 +170,12 @@ static_assert((uint64_t)TWO32_MOD_P == (1ull << 32) - 2ull * P && TWO32_MOD_P ==
 // non-negative value below 2^62 with the same residue.
 constexpr uint64_t P_SHIFT29 = (uint64_t)P << 29;
 
-__host__ __device__ __forceinline__ int32_t centered(uint32_t r) {  // r in [0, p)
+__host__ __device__ __forceinline__ int32_t centered(uint32_t r) {  // r in [0, p + 2^28)
     return (int32_t)(r > HALF_P ? r - P : r);
 }
+// any u32 -> its centered residue: one subtract-min leaves [0, 2^32 - p) =
+// [0, p + 2^28 - 2), whose part past p is already below (p-1)/2 after - p
+__device__ __forceinline__ int32_t centered_any(uint32_t v) { return centered(reduce_2p(v)); }
 __device__ __forceinline__ int64_t sfold(int64_t a) {
     const int64_t h = a >> 32;  // floor(a / 2^32)
     return (h << 28) - (h << 1) + (int64_t)(uint32_t)a;
@@ -181,15 +185,24 @@ __device__ __forceinline__ uint64_t fold32(uint64_t a) {
     return (uint64_t)(uint32_t)(a >> 32) * TWO32_MOD_P + (uint32_t)a;
 }
 
-// Centered copy of the coefficient limbs (a caller's table may hold any u32)
-// in four planes: plane j holds, for every column quad q, the four limbs of
-// column 4q + j, so one plane of a column chunk is one contiguous copy.
-__global__ void k_rlc_prep(const uint4* __restrict__ coeff, uint64_t quads, int4* __restrict__ w) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < 4 * quads;
+// Centered copies of the coefficient limbs (a caller's table may hold any u32):
+//   planar  four planes, plane j holding for every column quad q the limbs of
+//           column 4q + j, so one plane of a column chunk is one contiguous copy
+//           (the few-rows kernel);
+//   rowwise [column][limb] padded with zero columns to npad, a multiple of the
+//           row kernel's 32-column chunk.
+// A null table pointer skips that layout.
+__global__ void k_rlc_prep(const uint4* __restrict__ coeff, uint64_t quads, uint64_t npad, int4* __restrict__ planar,
+                           int4* __restrict__ rowwise) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < npad;
          i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint4 c = coeff[i];
-        w[(i & 3) * quads + (i >> 2)] =
-            make_int4(centered(c.x % P), centered(c.y % P), centered(c.z % P), centered(c.w % P));
+        int4 w = make_int4(0, 0, 0, 0);
+        if (i < 4 * quads) {
+            const uint4 c = coeff[i];
+            w = make_int4(centered(c.x % P), centered(c.y % P), centered(c.z % P), centered(c.w % P));
+            if (planar) planar[(i & 3) * quads + (i >> 2)] = w;
+        }
+        if (rowwise) rowwise[i] = w;
     }
 }
 
@@ -321,11 +334,14 @@ __global__ void __launch_bounds__(rlcb::THREADS, 1) k_rlc_rows(const uint32_t* _
     uint32_t rb = rb0, ph = 0;
     uint64_t ch = ch0;
     int s = 0;
+    // A warp whose wait gives up flags the error and from then on only keeps
+    // step: it arrives on `empty` and joins the flushes, so no barrier is left
+    // short and every other warp finishes its units.
+    bool dead = false;
     for (uint64_t u = u0; u < u1; u++) {
-        const bool ok = mbar_wait_bounded(&full[s], ph);
-        if (group_vote_or(bar, !ok, 256)) {
-            if (t == 0) atomicOr(err, 1);
-            return;
+        if (!dead && !__all_sync(0xFFFFFFFFu, mbar_wait_bounded(&full[s], ph))) {
+            dead = true;
+            if (lane == 0) atomicOr(err, 1);
         }
         const uint32_t rg = rb * UROWS + g * RPT;  // this group's first row
         const uint64_t qb = ch * CHQ;
@@ -334,7 +350,7 @@ __global__ void __launch_bounds__(rlcb::THREADS, 1) k_rlc_rows(const uint32_t* _
 #pragma unroll
         for (int k = 0; k < QPU; k++) {
             const int qi = k * 256 + t;
-            if (qb + qi >= quads) break;
+            if (dead || qb + qi >= quads) break;
             int4 w[4];
 #pragma unroll
             for (int j = 0; j < 4; j++) w[j] = sc[j * CHQ + qi];
@@ -342,8 +358,7 @@ __global__ void __launch_bounds__(rlcb::THREADS, 1) k_rlc_rows(const uint32_t* _
             for (int r = 0; r < RPT; r++) {
                 if (rg + r >= rows) break;
                 const uint4 v = sx[(g * RPT + r) * CHQ + qi];
-                const int32_t xv[4] = {centered(reduce_2p(reduce_2p(v.x))), centered(reduce_2p(reduce_2p(v.y))),
-                                       centered(reduce_2p(reduce_2p(v.z))), centered(reduce_2p(reduce_2p(v.w)))};
+                const int32_t xv[4] = {centered_any(v.x), centered_any(v.y), centered_any(v.z), centered_any(v.w)};
 #pragma unroll
                 for (int l = 0; l < 4; l++)
 #pragma unroll
@@ -385,6 +400,166 @@ __global__ void __launch_bounds__(rlcb::THREADS, 1) k_rlc_rows(const uint32_t* _
     }
 }
 
+// ---- row kernel: one consumer thread per row ------------------------------------
+// For tall matrices. A unit is UROWS = 512 rows x 32 columns, two TMA boxes of
+// 256 rows x 128 bytes with the 128-byte swizzle (a row's 16-byte chunk j sits
+// at chunk j ^ (row & 7) of its 128-byte line, so the 8 rows a quarter-warp
+// reads fall in 8 distinct bank groups), plus the 32 columns' coefficients
+// (512 bytes, read by every thread at the same address: broadcasts). Thread t
+// owns rows t + 256 k of the unit and sums each over the unit's columns in
+// registers, so no cross-thread reduction exists: a flush is 4 atomics per row.
+// Rows and columns past the matrix arrive as TMA zero fill and the coefficient
+// table is zero-padded, so the last unit needs no special case. Units are
+// dealt as in the few-rows kernel (row block major, an equal share per CTA).
+namespace rlct {
+constexpr int BOX_C = 32;
+constexpr int BOX_R = 256;
+constexpr int CT = 256;  // consumer threads
+constexpr int UROWS = 2 * BOX_R;
+constexpr int RPT = UROWS / CT;
+constexpr int NST = 3;
+constexpr int X_BYTES = UROWS * BOX_C * 4;
+constexpr int C_BYTES = BOX_C * 16;
+constexpr int STAGE_BYTES = X_BYTES + 1024;  // coefficients after the boxes; keeps stages 1024-byte aligned
+constexpr int OFF_BAR = NST * STAGE_BYTES;
+constexpr int SMEM = OFF_BAR + 2 * NST * 8;
+constexpr int THREADS = CT + 32;
+static_assert(C_BYTES <= 1024, "coefficients fit the stage's tail");
+static_assert(SMEM <= 227 * 1024, "shared memory per CTA");
+static_assert(UROWS % CT == 0 && BOX_C % 8 == 0, "geometry");
+}  // namespace rlct
+
+__global__ void __launch_bounds__(rlct::THREADS, 1) k_rlc_rows_t(const __grid_constant__ CUtensorMap tm_x,
+                                                                 uint32_t rows, uint64_t cols,
+                                                                 const int4* __restrict__ cw,
+                                                                 unsigned long long* __restrict__ acc,
+                                                                 int* __restrict__ err) {
+    using namespace rlct;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + OFF_BAR);
+    uint64_t* empty = full + NST;
+    const int tid = threadIdx.x;
+    const uint64_t nch = (cols + BOX_C - 1) / BOX_C;
+    const uint64_t U = nch * ((rows + UROWS - 1) / UROWS);
+    const uint64_t u0 = U * blockIdx.x / gridDim.x, u1 = U * (blockIdx.x + 1) / gridDim.x;
+    if (tid == 0) {
+        for (int s = 0; s < NST; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], CT / 32);
+        }
+        fence_mbar_init();
+    }
+    __syncthreads();
+    const uint32_t rb0 = (uint32_t)(u0 / nch);
+    const uint64_t ch0 = u0 % nch;
+    if (tid >= CT) {  // producer warp, lane 0
+        if (tid != CT) return;
+        uint32_t rb = rb0, ph = 0;
+        uint64_t ch = ch0;
+        int s = 0;
+        bool reuse = false;
+        for (uint64_t u = u0; u < u1; u++) {
+            if (reuse) {
+                if (!mbar_wait_bounded(&empty[s], ph ^ 1)) {
+                    atomicOr(err, 4);
+                    return;
+                }
+                fence_proxy_async();
+            }
+            unsigned char* st = smem + s * STAGE_BYTES;
+            mbar_expect_tx(&full[s], X_BYTES + C_BYTES);
+            for (int b = 0; b < UROWS / BOX_R; b++)
+                tma_load_2d(st + b * BOX_R * BOX_C * 4, &tm_x, (int)(ch * BOX_C), (int)(rb * UROWS + b * BOX_R),
+                            &full[s]);
+            bulk_load_1d(st + X_BYTES, cw + ch * BOX_C, C_BYTES, &full[s]);
+            if (++s == NST) {
+                s = 0;
+                ph ^= 1;
+                reuse = true;
+            }
+            if (++ch == nch) {
+                ch = 0;
+                rb++;
+            }
+        }
+        return;
+    }
+    const int lane = tid & 31;
+    int64_t sum[RPT][4];
+#pragma unroll
+    for (int k = 0; k < RPT; k++)
+#pragma unroll
+        for (int l = 0; l < 4; l++) sum[k][l] = 0;
+    // this thread's rows in a unit: t + CT k, each in box (t + CT k) / BOX_R at line (t + CT k) % BOX_R
+    uint32_t line_off[RPT];
+#pragma unroll
+    for (int k = 0; k < RPT; k++) {
+        const int r = tid + CT * k;
+        line_off[k] = (uint32_t)((r / BOX_R) * BOX_R * BOX_C * 4 + (r % BOX_R) * BOX_C * 4);
+    }
+    const int swz = tid & 7;  // (row & 7) is the same for all of this thread's rows: CT and BOX_R are multiples of 8
+    uint32_t rb = rb0, ph = 0;
+    uint64_t ch = ch0;
+    int s = 0;
+    bool dead = false;  // as in the few-rows kernel: a warp that gave up a wait only keeps step
+    for (uint64_t u = u0; u < u1; u++) {
+        if (!dead && !__all_sync(0xFFFFFFFFu, mbar_wait_bounded(&full[s], ph))) {
+            dead = true;
+            if (lane == 0) atomicOr(err, 1);
+        }
+        if (!dead) {
+            const unsigned char* st = smem + s * STAGE_BYTES;
+            const int4* sc = reinterpret_cast<const int4*>(st + X_BYTES);
+#pragma unroll
+            for (int q = 0; q < BOX_C / 4; q++) {
+                int4 w[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) w[j] = sc[4 * q + j];
+#pragma unroll
+                for (int k = 0; k < RPT; k++) {
+                    const uint4 v = *reinterpret_cast<const uint4*>(st + line_off[k] + ((q ^ swz) << 4));
+                    const int32_t xv[4] = {centered_any(v.x), centered_any(v.y), centered_any(v.z),
+                                           centered_any(v.w)};
+#pragma unroll
+                    for (int l = 0; l < 4; l++)
+#pragma unroll
+                        for (int j = 0; j < 4; j++) sum[k][l] += (int64_t)xv[j] * limb(w[j], l);
+                }
+                if (q & 1) {  // eight products per sum since the last fold
+#pragma unroll
+                    for (int k = 0; k < RPT; k++)
+#pragma unroll
+                        for (int l = 0; l < 4; l++) sum[k][l] = sfold(sum[k][l]);
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
+        if (u + 1 == u1 || ch + 1 == nch) {
+#pragma unroll
+            for (int k = 0; k < RPT; k++) {
+                const uint32_t row = rb * UROWS + tid + CT * k;
+                if (row < rows) {
+#pragma unroll
+                    for (int l = 0; l < 4; l++)
+                        atomicAdd(acc + (uint64_t)row * 4 + l,
+                                  (unsigned long long)((uint64_t)(sum[k][l] + (int64_t)P_SHIFT29) % P));
+                }
+#pragma unroll
+                for (int l = 0; l < 4; l++) sum[k][l] = 0;
+            }
+        }
+        if (++s == NST) {
+            s = 0;
+            ph ^= 1;
+        }
+        if (++ch == nch) {
+            ch = 0;
+            rb++;
+        }
+    }
+}
+
 __global__ void k_rlc_final(const unsigned long long* __restrict__ acc, uint64_t n, uint32_t* __restrict__ out) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
         out[i] = (uint32_t)(acc[i] % P);
@@ -405,19 +580,37 @@ unsigned grid1(const zoda_ctx* ctx, uint64_t n) {
     return (unsigned)(g < 1 ? 1 : g > cap ? cap : g);
 }
 
-// rlc of rows [rows][cols] (pitch cols) into out [rows][4]; table w prepared.
-zoda_status rlc_rows(const zoda_ctx* ctx, const uint32_t* x, uint32_t rows, uint64_t cols, const int4* w,
-                     unsigned long long* acc, uint32_t* out, cudaStream_t st) {
+// From this many rows on, the row kernel (a thread per row) runs; below, the
+// few-rows kernel (a thread per column quad).
+constexpr uint32_t RLC_ROW_KERNEL_MIN_ROWS = 256;
+
+// Byte offset of the row-wise table in ctx->rlc_w, after the planar one.
+inline uint64_t rowwise_offset(uint64_t cols) { return (cols * 16 + 255) / 256 * 256; }
+inline uint64_t rowwise_cols(uint64_t cols) { return (cols + rlct::BOX_C - 1) / rlct::BOX_C * rlct::BOX_C; }
+
+// rlc of rows [rows][cols] (pitch cols) into out [rows][4]; tables prepared.
+zoda_status rlc_rows(const zoda_ctx* ctx, const uint32_t* x, uint32_t rows, uint64_t cols, unsigned long long* acc,
+                     uint32_t* out, cudaStream_t st) {
     ZB_CUDA(cudaMemsetAsync(acc, 0, (size_t)rows * 4 * sizeof(unsigned long long), st));
     const uint64_t quads = cols / 4;
     if (rows > 262140) {
         set_last_error_text("rlc: more than 262140 rows");
         return ZODA_ERR_UNSUPPORTED;
     }
-    if (quads) {
+    const unsigned char* tabs = (const unsigned char*)ctx->rlc_w.p;
+    if (quads && rows >= RLC_ROW_KERNEL_MIN_ROWS) {
+        CUtensorMap tm;
+        zoda_status s = make_map(&tm, x, cols, rows, cols * 4, rlct::BOX_C, rlct::BOX_R, CU_TENSOR_MAP_SWIZZLE_128B);
+        if (s != ZODA_OK) return s;
+        const uint64_t units = (cols + rlct::BOX_C - 1) / rlct::BOX_C * ((rows + rlct::UROWS - 1) / rlct::UROWS);
+        const unsigned g = (unsigned)std::min<uint64_t>(units, (uint64_t)ctx->sm_count);
+        k_rlc_rows_t<<<g, rlct::THREADS, rlct::SMEM, st>>>(
+            tm, rows, cols, (const int4*)(tabs + rowwise_offset(cols)), acc, ctx->d_err);
+        ZB_CUDA(cudaGetLastError());
+    } else if (quads) {
         const uint64_t units = (quads + rlcb::CHQ - 1) / rlcb::CHQ * ((rows + rlcb::UROWS - 1) / rlcb::UROWS);
         const unsigned g = (unsigned)std::min<uint64_t>(units, (uint64_t)ctx->sm_count);
-        k_rlc_rows<<<g, rlcb::THREADS, rlcb::SMEM, st>>>(x, cols, rows, quads, w, acc, ctx->d_err);
+        k_rlc_rows<<<g, rlcb::THREADS, rlcb::SMEM, st>>>(x, cols, rows, quads, (const int4*)tabs, acc, ctx->d_err);
         ZB_CUDA(cudaGetLastError());
     }
     k_rlc_final<<<grid1(ctx, (uint64_t)rows * 4), 256, 0, st>>>(acc, (uint64_t)rows * 4, out);
@@ -425,10 +618,20 @@ zoda_status rlc_rows(const zoda_ctx* ctx, const uint32_t* x, uint32_t rows, uint
     return ZODA_OK;
 }
 
-zoda_status prep_tables(zoda_ctx* ctx, const uint32_t* d_coeff, uint64_t cols, cudaStream_t st) {
+// Coefficient tables for RLCs of `rows_a` and `rows_b` rows (0: none): only the
+// layouts the kernels for those row counts read.
+zoda_status prep_tables(zoda_ctx* ctx, const uint32_t* d_coeff, uint64_t cols, uint32_t rows_a, uint32_t rows_b,
+                        cudaStream_t st) {
     zoda_status s;
-    if ((s = ctx->rlc_w.ensure(cols * 16 + 16)) != ZODA_OK) return s;
-    k_rlc_prep<<<grid1(ctx, cols), 256, 0, st>>>((const uint4*)d_coeff, cols / 4, (int4*)ctx->rlc_w.p);
+    const uint64_t npad = rowwise_cols(cols);
+    if ((s = ctx->rlc_w.ensure(rowwise_offset(cols) + npad * 16)) != ZODA_OK) return s;
+    unsigned char* tabs = (unsigned char*)ctx->rlc_w.p;
+    auto row_kernel = [](uint32_t r) { return r >= RLC_ROW_KERNEL_MIN_ROWS; };
+    const bool planar = (rows_a && !row_kernel(rows_a)) || (rows_b && !row_kernel(rows_b));
+    const bool rowwise = row_kernel(rows_a) || row_kernel(rows_b);
+    k_rlc_prep<<<grid1(ctx, npad), 256, 0, st>>>((const uint4*)d_coeff, cols / 4, rowwise ? npad : cols,
+                                                 planar ? (int4*)tabs : nullptr,
+                                                 rowwise ? (int4*)(tabs + rowwise_offset(cols)) : nullptr);
     ZB_CUDA(cudaGetLastError());
     return ZODA_OK;
 }
@@ -437,6 +640,7 @@ zoda_status prep_tables(zoda_ctx* ctx, const uint32_t* d_coeff, uint64_t cols, c
 
 zoda_status rlc_init_attributes() {
     ZB_CUDA(cudaFuncSetAttribute(k_rlc_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, rlcb::SMEM));
+    ZB_CUDA(cudaFuncSetAttribute(k_rlc_rows_t, cudaFuncAttributeMaxDynamicSharedMemorySize, rlct::SMEM));
     return ZODA_OK;
 }
 
@@ -505,11 +709,10 @@ zoda_status zoda_rlc_rows_device(zoda_ctx* ctx, const uint32_t* d_rows, uint32_t
     ZB_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t st = (cudaStream_t)stream;
     std::lock_guard<std::mutex> lock(ctx->rlc_mu);
-    zoda_status s = prep_tables(ctx, d_coeff, cols, st);
+    zoda_status s = prep_tables(ctx, d_coeff, cols, rows, 0, st);
     if (s != ZODA_OK) return s;
     if ((s = ctx->rlc_acc.ensure((size_t)rows * 4 * 8)) != ZODA_OK) return s;
-    return rlc_rows(ctx, d_rows, rows, cols, (const int4*)ctx->rlc_w.p,
-                    (unsigned long long*)ctx->rlc_acc.p, d_out, st);
+    return rlc_rows(ctx, d_rows, rows, cols, (unsigned long long*)ctx->rlc_acc.p, d_out, st);
 }
 
 zoda_status zoda_rlc_check_device(zoda_ctx* ctx, const uint32_t* d_data, const uint32_t* d_code, uint32_t k,
@@ -521,20 +724,19 @@ zoda_status zoda_rlc_check_device(zoda_ctx* ctx, const uint32_t* d_data, const u
     cudaStream_t st = (cudaStream_t)stream;
     const uint32_t rows = k + n;
     std::lock_guard<std::mutex> lock(ctx->rlc_mu);
-    zoda_status s = prep_tables(ctx, d_coeff, cols, st);
+    zoda_status s = prep_tables(ctx, d_coeff, cols, k, rows, st);
     if (s != ZODA_OK) return s;
     if ((s = ctx->rlc_acc.ensure((size_t)rows * 4 * 8)) != ZODA_OK) return s;
     if ((s = ctx->rlc_d.ensure((size_t)k * 16)) != ZODA_OK) return s;
     if ((s = ctx->rlc_e.ensure((size_t)rows * 16)) != ZODA_OK) return s;
     if ((s = ctx->rlc_f.ensure((size_t)rows * 16)) != ZODA_OK) return s;
     if ((s = ctx->rlc_cnt.ensure(8)) != ZODA_OK) return s;
-    const int4* w = (const int4*)ctx->rlc_w.p;
     unsigned long long* acc = (unsigned long long*)ctx->rlc_acc.p;
     uint32_t *D = (uint32_t*)ctx->rlc_d.p, *E = (uint32_t*)ctx->rlc_e.p, *F = (uint32_t*)ctx->rlc_f.p;
-    if ((s = rlc_rows(ctx, d_data, k, cols, w, acc, D, st)) != ZODA_OK) return s;
+    if ((s = rlc_rows(ctx, d_data, k, cols, acc, D, st)) != ZODA_OK) return s;
     // the RLC and the extension commute (both F_p-linear): extend the k x 4 RLC matrix
     if ((s = zoda_encode_device(ctx, D, F, k, n, 4, st)) != ZODA_OK) return s;
-    if ((s = rlc_rows(ctx, d_code, rows, cols, w, acc, E, st)) != ZODA_OK) return s;
+    if ((s = rlc_rows(ctx, d_code, rows, cols, acc, E, st)) != ZODA_OK) return s;
     ZB_CUDA(cudaMemsetAsync(ctx->rlc_cnt.p, 0, 8, st));
     k_count_diff<<<grid1(ctx, (uint64_t)rows * 4), 256, 0, st>>>(E, F, (uint64_t)rows * 4,
                                                                 (unsigned long long*)ctx->rlc_cnt.p);
