@@ -656,8 +656,17 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=10.0, help="seconds of CPU baseline sampling")
     ap.add_argument("--ref-step-budget", type=float, default=None,
                     help="seconds of CPU work per step of --impl reference (default: about 60 s in total)")
+    ap.add_argument("--leg", choices=["rlc", "recover", "encode"], default=None,
+                    help="run one report-only leg on one GPU and print its JSON (a small case to profile)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps
+    if args.leg:
+        import zoda_b200
+        ctx = zoda_b200.Context(0)
+        leg = {"rlc": lambda: time_rlc(ctx, 1024), "recover": lambda: time_recover(ctx, 1024),
+               "encode": lambda: time_encode_general(ctx, 1000, 1000)}[args.leg]
+        print(json.dumps({"leg": args.leg, **leg()}))
+        return
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
