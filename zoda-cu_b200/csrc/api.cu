@@ -129,16 +129,18 @@ static void build_side_tables(int ls, int lept, std::vector<Tw>& all, size_t off
 
 // Copies input row m to output row 2m for every m on a few host threads, from
 // construction until join() (or destruction, on an early error return).
+// Copies columns [0, ncopy) of every input row m to output row 2m on host threads.
 class EvenRowCopy {
    public:
-    EvenRowCopy(const uint32_t* in, uint32_t* out, uint32_t k, uint64_t cols) {
+    EvenRowCopy(const uint32_t* in, uint32_t* out, uint32_t k, uint64_t cols, uint64_t ncopy) {
+        if (ncopy == 0) return;
         unsigned n = std::thread::hardware_concurrency() / 2;
         n = n < 1 ? 1 : n > 16 ? 16 : n;
         if (n > k) n = k;
         for (unsigned t = 0; t < n; t++)
             th_.emplace_back([=] {
                 for (uint64_t m = (uint64_t)k * t / n; m < (uint64_t)k * (t + 1) / n; m++)
-                    memcpy(out + 2 * m * cols, in + m * cols, cols * 4);
+                    memcpy(out + 2 * m * cols, in + m * cols, ncopy * 4);
             });
     }
     void join() {
@@ -150,6 +152,10 @@ class EvenRowCopy {
    private:
     std::vector<std::thread> th_;
 };
+
+// Share of the column chunks of a host call whose even output rows return
+// over PCIe rather than through the host copy (measured on B200 hosts).
+constexpr double HOST_EVEN_DEVICE_SHARE = 0.125;
 
 static int log2_exact(uint64_t x) {
     if (x == 0 || (x & (x - 1))) return -1;
@@ -330,11 +336,6 @@ zoda_status zoda_extend_host(zoda_ctx* ctx, const uint32_t* h_in, uint32_t* h_ou
         return ZODA_OK;
     }
     const auto t_start = std::chrono::steady_clock::now();
-    // The even output rows are the input rows (the code is systematic), so
-    // they never cross PCIe: host threads copy them while the GPU computes
-    // the odd rows, which come back compactly. PCIe carries k*cols words each
-    // way instead of k*cols up and 2*k*cols down.
-    EvenRowCopy even(h_in, h_out, k, cols);
     // Column chunks of ~64 MiB input rotate over NHS streams, so the upload of
     // one chunk, the kernel of another and the download of a third overlap
     // (the two copy directions run on separate engines).
@@ -345,6 +346,17 @@ zoda_status zoda_extend_host(zoda_ctx* ctx, const uint32_t* h_in, uint32_t* h_ou
     uint64_t cw = (cols + nch - 1) / nch;
     cw = (cw + 3) & ~3ull;
     nch = (cols + cw - 1) / cw;
+    // The even output rows are the input rows (the code is systematic): host
+    // threads copy them from h_in while the GPU computes the odd rows, which
+    // come back compactly. The host copy is the slower of the two (host memory
+    // bandwidth; PCIe has time to spare), so the even rows of the last
+    // dev_even chunks come back over PCIe instead, from the device's copy of
+    // the input: PCIe carries k*cols words up and (1 + dev_even/nch)*k*cols
+    // down, instead of k*cols up and 2*k*cols down.
+    uint64_t dev_even = (uint64_t)(nch * HOST_EVEN_DEVICE_SHARE + 0.5);
+    if (dev_even >= nch) dev_even = nch - 1;
+    const uint64_t host_cols = (nch - dev_even) * cw < cols ? (nch - dev_even) * cw : cols;
+    EvenRowCopy even(h_in, h_out, k, cols, host_cols);
     for (int i = 0; i < zoda_ctx::NHS; i++) {
         if (!ctx->hs[i]) ZB_CUDA(cudaStreamCreateWithFlags(&ctx->hs[i], cudaStreamNonBlocking));
         if ((s = ctx->hin[i].ensure((size_t)k * cw * 4)) != ZODA_OK) return s;
@@ -371,6 +383,9 @@ zoda_status zoda_extend_host(zoda_ctx* ctx, const uint32_t* h_in, uint32_t* h_ou
         // odd rows 1, 3, .. of the output: a stride of two output rows
         ZB_CUDA(cudaMemcpy2DAsync(h_out + cols + c0, 2 * cols * 4, dout, w * 4, w * 4, (size_t)k,
                                   cudaMemcpyDeviceToHost, st));
+        if (c0 >= host_cols)  // even rows 0, 2, .. of this chunk: the uploaded input, before the buffer is reused
+            ZB_CUDA(cudaMemcpy2DAsync(h_out + c0, 2 * cols * 4, din, w * 4, w * 4, (size_t)k,
+                                      cudaMemcpyDeviceToHost, st));
         ZB_CUDA(cudaEventRecord(e[3], st));
     }
     for (int i = 1; i < zoda_ctx::NHS; i++) {

@@ -414,7 +414,7 @@ __global__ void __launch_bounds__(rlcb::THREADS, 1) k_rlc_rows(const uint32_t* _
 namespace rlct {
 constexpr int BOX_C = 32;
 constexpr int BOX_R = 256;
-constexpr int CT = 256;  // consumer threads
+constexpr int CT = 512;  // consumer threads
 constexpr int UROWS = 2 * BOX_R;
 constexpr int RPT = UROWS / CT;
 constexpr int NST = 3;
