@@ -406,7 +406,7 @@ __global__ void __launch_bounds__(rlcb::THREADS, 1) k_rlc_rows(const uint32_t* _
 // at chunk j ^ (row & 7) of its 128-byte line, so the 8 rows a quarter-warp
 // reads fall in 8 distinct bank groups), plus the 32 columns' coefficients
 // (512 bytes, read by every thread at the same address: broadcasts). Thread t
-// owns rows t + 256 k of the unit and sums each over the unit's columns in
+// owns rows t + CT k of the unit and sums each over the unit's columns in
 // registers, so no cross-thread reduction exists: a flush is 4 atomics per row.
 // Rows and columns past the matrix arrive as TMA zero fill and the coefficient
 // table is zero-padded, so the last unit needs no special case. Units are
