@@ -81,4 +81,83 @@ __global__ void __launch_bounds__(LEPT == 3 ? 1024 : 512, 1)
     }
 }
 
+// Two transforms in one pass, the decoder's building block:
+//   out[r] = NTT_N( mid(i) * INTT_N( pre(j) * in[j] )(i) )(r)
+// with the INTT unscaled (mid carries any 1/N), rows j >= in_rows or with a
+// zero pre-factor never read, and the product staying in registers between
+// the transforms (the fused extension's INTT -> twist -> NTT with tables in
+// place of g^i / S). OSH = 1 stores only the even outputs r = 2m, at row m:
+// the k-point NTT of coefficients zero-padded to N = 2k. With `counter`, the
+// INTT coefficients i >= count_from that are nonzero are counted (before mid).
+struct ColTx2 {
+    const uint32_t* in;
+    uint64_t in_pitch;
+    uint32_t in_rows;
+    const uint2* pre;  // per input row
+    const Tw* mid;     // per coefficient index, N entries
+    uint32_t* out;
+    uint64_t out_pitch;
+    uint32_t out_rows;  // outputs r >= out_rows are not stored
+    uint64_t cols;      // multiple of 4
+    uint32_t count_from;
+    unsigned long long* counter;  // or nullptr
+};
+
+template <int LOG_N, int LEPT, int OSH, bool COUNT>
+__global__ void __launch_bounds__(LEPT == 3 ? 1024 : 512, 1)
+    k_coltx2(const ColTx2 a, uint64_t ntiles, const Tw* __restrict__ tw) {
+    using PL = ExtPlan<LOG_N, 0, LEPT, LEPT == 3 ? 1024 : 512>;
+    extern __shared__ uint4 sm[];
+    const int tid = threadIdx.x;
+    const int q = tid % PL::Q4;
+    const int t = tid / PL::Q4;
+    const OddOut oo{a.out, a.out_pitch, a.out_rows};
+    unsigned long long cnt = 0;
+    V4 v[PL::EPT];
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint64_t col = tile * PL::C + 4 * (uint64_t)q;
+        const bool active = col < a.cols;
+        constexpr int R0 = 1 << PL::lr(0);
+        constexpr int G0 = PL::EPT / R0;
+        constexpr int L0 = PL::S / R0;
+#pragma unroll
+        for (int g = 0; g < G0; g++)
+#pragma unroll
+            for (int j = 0; j < R0; j++) {
+                const uint32_t row = (uint32_t)(g * PL::TPQ + t) + (uint32_t)L0 * j;
+                const uint2 u = row < a.in_rows ? __ldg(a.pre + row) : make_uint2(0u, 0u);
+                if (active && u.x != 0) {
+                    v[g * R0 + j] = ldg_stream_v4(a.in + (uint64_t)row * a.in_pitch + col);
+                    mul4(v[g * R0 + j], Tw{u.x, u.y});
+                } else {
+                    v[g * R0 + j] = V4{{0, 0, 0, 0}};
+                }
+            }
+        dif_levels<PL, 0, true>(v, sm, t, q, tw);
+        if constexpr (COUNT) {
+            // the INTT's last level: group g holds coefficients c0 + (S/R) j at v[g R + bitrev(j)]
+            constexpr int LR = PL::lr(PL::NLEV - 1);
+            constexpr int R = 1 << LR;
+            constexpr int SH = PL::LOG_S - LR;
+#pragma unroll
+            for (int g = 0; g < PL::EPT / R; g++) {
+                const uint32_t c0 = digit_rev<PL, false>((uint32_t)(g * PL::TPQ + t) << LR);
+#pragma unroll
+                for (int j = 0; j < R; j++) {
+                    const V4& x = v[g * R + bitrev(j, LR)];
+                    if (active && c0 + ((uint32_t)j << SH) >= a.count_from)
+#pragma unroll
+                        for (int e = 0; e < 4; e++) cnt += x.c[e] % P != 0;
+                }
+            }
+        }
+        twist_and_first_ntt<PL, OSH>(v, sm, t, q, tw, a.mid, oo, col, active);
+    }
+    if constexpr (COUNT) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xFFFFFFFFu, cnt, o);
+        if ((tid & 31) == 0 && cnt) atomicAdd(a.counter, cnt);
+    }
+}
+
 }  // namespace zb

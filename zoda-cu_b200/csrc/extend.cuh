@@ -166,7 +166,9 @@ struct OddOut {
     uint32_t rows;
 };
 
-template <class PL, int l>
+// OSH > 0 (the decoder's last pass): only outputs k with k % 2^OSH == 0 are
+// stored, at row k >> OSH.
+template <class PL, int l, int OSH = 0>
 __device__ __forceinline__ void ntt_levels(V4* v, uint4* sm, int t, int q, const Tw* tw,
                                            const OddOut& oo, uint64_t col, bool active) {
     using LV = Level<PL, PL::nlr(l), PL::npre(l)>;
@@ -175,7 +177,7 @@ __device__ __forceinline__ void ntt_levels(V4* v, uint4* sm, int t, int q, const
     if constexpr (l < PL::NLEV - 1) {
         LV::template twiddle_write<false>(v, sm, t, q, tw);
         __syncthreads();
-        ntt_levels<PL, l + 1>(v, sm, t, q, tw, oo, col, active);
+        ntt_levels<PL, l + 1, OSH>(v, sm, t, q, tw, oo, col, active);
     } else {
         // last level: L = 1, slot = block*R + k2 -> output index by digit reversal
 #pragma unroll
@@ -184,7 +186,8 @@ __device__ __forceinline__ void ntt_levels(V4* v, uint4* sm, int t, int q, const
 #pragma unroll
             for (int r = 0; r < LV::R; r++) {
                 const uint32_t k = digit_rev<PL, true>((blk << PL::nlr(l)) + (uint32_t)bitrev(r, PL::nlr(l)));
-                if (active && k < oo.rows) stg_stream_v4(oo.p + (uint64_t)k * oo.stride + col, v[g * LV::R + r]);
+                if (active && k < oo.rows && (k & ((1u << OSH) - 1)) == 0)
+                    stg_stream_v4(oo.p + (uint64_t)(k >> OSH) * oo.stride + col, v[g * LV::R + r]);
             }
         }
     }
@@ -195,7 +198,7 @@ __device__ __forceinline__ void ntt_levels(V4* v, uint4* sm, int t, int q, const
 // slots b*R + k2, i.e. coefficients c0 + (S/R)*k2 with c0 = digit_rev(b*R).
 // The NTT's first level (radix R over stride S/R) needs exactly those
 // coefficients, in natural k2 order, as group n1 = c0.
-template <class PL>
+template <class PL, int OSH = 0>
 __device__ __forceinline__ void twist_and_first_ntt(V4* v, uint4* sm, int t, int q, const Tw* tw,
                                                     const Tw* __restrict__ twist, const OddOut& oo, uint64_t col,
                                                     bool active) {
@@ -234,13 +237,14 @@ __device__ __forceinline__ void twist_and_first_ntt(V4* v, uint4* sm, int t, int
             }
         }
         __syncthreads();
-        ntt_levels<PL, 1>(v, sm, t, q, tw, oo, col, active);
+        ntt_levels<PL, 1, OSH>(v, sm, t, q, tw, oo, col, active);
     } else {
         // single level: output index k2 = bitrev(r)
 #pragma unroll
         for (int r = 0; r < R; r++) {
             const uint32_t k = (uint32_t)bitrev(r, LR);
-            if (active && k < oo.rows) stg_stream_v4(oo.p + (uint64_t)k * oo.stride + col, v[r]);
+            if (active && k < oo.rows && (k & ((1u << OSH) - 1)) == 0)
+                stg_stream_v4(oo.p + (uint64_t)(k >> OSH) * oo.stride + col, v[r]);
         }
     }
 }

@@ -21,7 +21,11 @@
 //   row = NTT_k(F~_i * h^-i), i < k                     f at omega_k^m = data row m
 // with h = 31 (a generator of F_p^*, never a 2k-th root of unity, so Z(h w) != 0).
 // F~_i must vanish for i >= k when the known rows are one codeword; the
-// optional check counts the entries that do not.
+// optional check counts the entries that do not. The four transforms run as two
+// fused passes (k_coltx2), each an INTT and an NTT with the pointwise factor
+// between them applied in registers: pass A gives g~, pass B gives the data
+// rows as the even outputs of NTT_2k(F~_i * h^-i, zero for i >= k), which is
+// NTT_k of the first k coefficients at omega_2k^(2m) = omega_k^m.
 #include <algorithm>
 #include <vector>
 
@@ -75,6 +79,36 @@ zoda_status coltx(const zoda_ctx* ctx, int log_n, bool inv, const ColTx& a, cuda
     }
 }
 
+template <int LOG_N, int OSH, bool COUNT>
+zoda_status coltx2_t(const zoda_ctx* ctx, const ColTx2& a, cudaStream_t st) {
+    constexpr int LEPT = LOG_N >= 9 ? 3 : 4;
+    using PL = ExtPlan<LOG_N, 0, LEPT, LEPT == 3 ? 1024 : 512>;
+    const uint64_t ntiles = (a.cols + PL::C - 1) / PL::C;
+    if (ntiles == 0 || a.out_rows == 0) return ZODA_OK;
+    if (PL::SMEM > 0)
+        ZB_CUDA(cudaFuncSetAttribute(k_coltx2<LOG_N, LEPT, OSH, COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)PL::SMEM));
+    const uint64_t grid = ntiles < (uint64_t)ctx->sm_count ? ntiles : (uint64_t)ctx->sm_count;
+    k_coltx2<LOG_N, LEPT, OSH, COUNT><<<(unsigned)grid, PL::THREADS, PL::SMEM, st>>>(a, ntiles, ctx->tables.tw);
+    ZB_CUDA(cudaGetLastError());
+    return ZODA_OK;
+}
+
+// INTT -> mid -> NTT of size 2^log_n (1 <= log_n <= 13) in one pass; even_out
+// stores only the even outputs (row r / 2); a.counter selects the counting form.
+zoda_status coltx2(const zoda_ctx* ctx, int log_n, bool even_out, const ColTx2& a, cudaStream_t st) {
+    switch (log_n) {
+#define ZB_CASE(L)                                                                       \
+    case L:                                                                              \
+        if (!even_out) return coltx2_t<L, 0, false>(ctx, a, st);                         \
+        return a.counter ? coltx2_t<L, 1, true>(ctx, a, st) : coltx2_t<L, 1, false>(ctx, a, st);
+        ZB_CASE(1) ZB_CASE(2) ZB_CASE(3) ZB_CASE(4) ZB_CASE(5) ZB_CASE(6)
+        ZB_CASE(7) ZB_CASE(8) ZB_CASE(9) ZB_CASE(10) ZB_CASE(11) ZB_CASE(12) ZB_CASE(13)
+#undef ZB_CASE
+        default: return ZODA_ERR_UNSUPPORTED;
+    }
+}
+
 // out[r * pitch + c] = in[c] for r in [0, rows), c in [0, cols).
 __global__ void k_bcast_rows(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint64_t pitch,
                              uint32_t rows, uint64_t cols) {
@@ -100,13 +134,13 @@ __device__ __forceinline__ uint2 shoup_pair_dev(uint32_t w) {
 
 // Decoder tables for one erasure pattern over N = 2^log_n points (see the top
 // of this file); roots[e] = omega_N^e for the erased e:
-//   zk[j]  = Z(omega^j)          (0 at erased j)
-//   hp[i]  = h^i
-//   izh[j] = 1 / Z(h * omega^j)
-//   hm[i]  = h^-i
+//   zk[j]    = Z(omega^j)          (0 at erased j)
+//   izh[j]   = 1 / Z(h * omega^j)
+//   mid_a[i] = h^i / N
+//   mid_b[i] = h^-i / N for i < k, else 0
 __global__ void k_erasure_tables(const uint32_t* __restrict__ erased_roots, uint32_t ne, int log_n,
-                                 const Tw* __restrict__ tw, uint2* __restrict__ zk, uint2* __restrict__ hp,
-                                 uint2* __restrict__ izh, uint2* __restrict__ hm) {
+                                 const Tw* __restrict__ tw, uint32_t k, uint32_t ninv, uint2* __restrict__ zk,
+                                 uint2* __restrict__ izh, uint2* __restrict__ mid_a, uint2* __restrict__ mid_b) {
     const uint32_t N = 1u << log_n;
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= N) return;
@@ -120,23 +154,11 @@ __global__ void k_erasure_tables(const uint32_t* __restrict__ erased_roots, uint
     }
     zk[j] = shoup_pair_dev(zx);
     izh[j] = shoup_pair_dev(pow_slow(zy, P - 2));
+    // the coset shift g^j and its inverse, with the INTTs' 1/N; coefficients
+    // j >= k of the quotient are dropped (zero) before the last NTT
     const uint32_t hj = pow_slow(GENERATOR, j);
-    hp[j] = shoup_pair_dev(hj);
-    hm[j] = shoup_pair_dev(pow_slow(hj, P - 2));
-}
-
-// *count += number of nonzero entries of rows [0, rows) x cols (pitch elements apart)
-__global__ void k_count_nonzero(const uint32_t* __restrict__ a, uint64_t pitch, uint32_t rows, uint64_t cols,
-                                unsigned long long* __restrict__ count) {
-    const uint64_t n = (uint64_t)rows * cols;
-    unsigned long long c = 0;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t r = i / cols, cc = i - r * cols;
-        c += a[r * pitch + cc] != 0;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xFFFFFFFFu, c, o);
-    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+    mid_a[j] = shoup_pair_dev(mul_slow(hj, ninv));
+    mid_b[j] = j < k ? shoup_pair_dev(mul_slow(pow_slow(hj, P - 2), ninv)) : make_uint2(0u, 0u);
 }
 
 unsigned grid_for(const zoda_ctx* ctx, uint64_t n) {
@@ -329,7 +351,7 @@ zoda_status zoda_recover_device(zoda_ctx* ctx, const uint32_t* d_code, const uin
         ZB_CUDA(cudaMemcpy2DAsync(d_data, rb, d_code, 2 * rb, rb, k, cudaMemcpyDeviceToDevice, st));
         return finish(ZODA_OK);
     }
-    // pattern tables: roots of the erased points, then zk | hp | izh | hm
+    // pattern tables: roots of the erased points, then zk | izh | mid_a | mid_b
     std::vector<uint32_t> er;
     const uint32_t wn = root_of_unity(ln);
     for (uint32_t j = 0, x = 1; j < N; j++, x = mulmod_c(x, wn))
@@ -337,39 +359,27 @@ zoda_status zoda_recover_device(zoda_ctx* ctx, const uint32_t* d_code, const uin
     if ((s = ctx->gen_tab.ensure((size_t)4 * N * sizeof(uint2))) != ZODA_OK) return finish(s);
     if ((s = ctx->gen_small.ensure(std::max<size_t>(1, er.size()) * 4 + 64)) != ZODA_OK) return finish(s);
     uint2* T = (uint2*)ctx->gen_tab.p;
-    uint2 *zk = T, *hp = T + N, *izh = T + 2 * N, *hm = T + 3 * N;
+    uint2 *zk = T, *izh = T + N, *mid_a = T + 2 * N, *mid_b = T + 3 * N;
     uint32_t* d_er = (uint32_t*)ctx->gen_small.p;
     unsigned long long* d_cnt = (unsigned long long*)((char*)ctx->gen_small.p + ((er.size() * 4 + 15) / 16) * 16);
     if (!er.empty())
         ZB_CUDA(cudaMemcpyAsync(d_er, er.data(), er.size() * 4, cudaMemcpyHostToDevice, st));
-    k_erasure_tables<<<(N + 127) / 128, 128, 0, st>>>(d_er, (uint32_t)er.size(), ln, ctx->tables.tw, zk, hp, izh, hm);
+    const uint32_t ninv = powmod_c(N, P - 2);
+    k_erasure_tables<<<(N + 127) / 128, 128, 0, st>>>(d_er, (uint32_t)er.size(), ln, ctx->tables.tw, k, ninv, zk,
+                                                      izh, mid_a, mid_b);
     ZB_CUDA(cudaGetLastError());
     if (mismatch) ZB_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), st));
     const uint64_t w0 = chunk_cols(cols, N);
     if ((s = ctx->gen_a.ensure((uint64_t)N * w0 * 4)) != ZODA_OK) return finish(s);
-    if ((s = ctx->gen_b.ensure((uint64_t)N * w0 * 4)) != ZODA_OK) return finish(s);
     uint32_t* A = (uint32_t*)ctx->gen_a.p;
-    uint32_t* B = (uint32_t*)ctx->gen_b.p;
-    const uint32_t ninv = powmod_c(N, P - 2);
-    const Tw sc_inv{ninv, shoup(ninv)}, one{1u, shoup(1u)};
     for (uint64_t c0 = 0; c0 < cols; c0 += w0) {
         const uint64_t w = std::min(w0, cols - c0);
-        const ColTx p1{d_code + c0, cols, N, zk, A, w, N, nullptr, sc_inv, w};
-        const ColTx p2{A, w, N, hp, B, w, N, nullptr, one, w};
-        const ColTx p3{B, w, N, izh, A, w, mismatch ? N : k, nullptr, sc_inv, w};
-        if ((s = coltx(ctx, ln, true, p1, st)) != ZODA_OK) return finish(s);
-        if ((s = coltx(ctx, ln, false, p2, st)) != ZODA_OK) return finish(s);
-        if ((s = coltx(ctx, ln, true, p3, st)) != ZODA_OK) return finish(s);
-        if (lk == 0) {
-            ZB_CUDA(cudaMemcpy2DAsync(d_data + c0, rb, A, w * 4, w * 4, 1, cudaMemcpyDeviceToDevice, st));
-        } else {
-            const ColTx p4{A, w, k, hm, d_data + c0, cols, k, nullptr, one, w};
-            if ((s = coltx(ctx, lk, false, p4, st)) != ZODA_OK) return finish(s);
-        }
-        if (mismatch) {
-            k_count_nonzero<<<grid_for(ctx, (uint64_t)k * w), 256, 0, st>>>(A + (uint64_t)k * w, w, k, w, d_cnt);
-            ZB_CUDA(cudaGetLastError());
-        }
+        // pass A: g~ = NTT(h^i / N * INTT(y * Z)) into the scratch
+        const ColTx2 pa{d_code + c0, cols, N, zk, (const Tw*)mid_a, A, w, N, w, 0, nullptr};
+        // pass B: data row m = even output 2m of NTT(h^-i / N [i < k] * INTT(g~ / Z(h w)))
+        const ColTx2 pb{A, w, N, izh, (const Tw*)mid_b, d_data + c0, cols, N, w, k, mismatch ? d_cnt : nullptr};
+        if ((s = coltx2(ctx, ln, false, pa, st)) != ZODA_OK) return finish(s);
+        if ((s = coltx2(ctx, ln, true, pb, st)) != ZODA_OK) return finish(s);
     }
     if (mismatch) {
         unsigned long long h = 0;
