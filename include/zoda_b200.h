@@ -303,8 +303,8 @@ zoda_status zoda_encode_device(zoda_ctx* ctx, const uint32_t* d_in, uint32_t* d_
  * nknown) are read, the others may hold anything. At least k distinct rows
  * must be known. d_data receives the original [k][cols] data. k is a power of
  * two <= 4096. When every even row is known the data is copied out; otherwise
- * the call runs four column transforms over 2k points (see general.cu) with
- * the context's scratch (<= 512 MiB). If `mismatch` is not NULL the call also
+ * the call runs two fused passes, each an INTT and an NTT over 2k points (see
+ * general.cu), with the context's scratch (<= 256 MiB). If `mismatch` is not NULL the call also
  * checks that the known rows are one codeword, stores the number of
  * inconsistent coefficients there (0 = consistent) and synchronizes `stream`;
  * otherwise it is asynchronous on `stream`. */
