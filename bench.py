@@ -255,7 +255,7 @@ def time_recover(ctx, k: int, reps: int = 5, seed: int = 3) -> dict:
     torch.cuda.empty_cache()
     return {"k": k, "cols": cols, "erased_rows": k, "ms": round(ms, 4),
             "gbps": round(payload_bits(k) / (ms * 1e-3) / 1e9, 1), "bit_exact": ok,
-            "api": "zoda_recover_device (two fused passes, each an INTT and an NTT over 2k points)"}
+            "api": "zoda_recover_device (two fused passes, each an INTT and an NTT over 2k points, TMA-staged)"}
 
 
 def time_rlc(ctx, k: int, reps: int = 5) -> dict:

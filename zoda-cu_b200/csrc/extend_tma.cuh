@@ -167,6 +167,15 @@ struct ConstTw {  // omega_{2^LOG_M}^(+-K), an immediate
     }
 };
 
+struct KTw {  // a per-k2 table: factor for output k2 = K is p[K]
+    const uint2* p;
+    template <int K>
+    __device__ __forceinline__ Tw get() const {
+        const uint2 u = __ldg(p + K);
+        return Tw{u.x, u.y};
+    }
+};
+
 namespace detail {
 template <int LR, bool SKIP0, int I, class TwF>
 __device__ __forceinline__ void pair_twout(V4* x, const TwF& twf) {
@@ -287,8 +296,8 @@ __device__ __forceinline__ void intt_upto_last(V4* v, uint2* xg, int t, int ql, 
 }
 
 // NTT levels l .. NLEV-1 (level 0 runs in the kernel body); the last one stores
-// the odd output rows.
-template <class TP, int l>
+// the odd output rows (OSH > 0: only outputs k % 2^OSH == 0, at row k >> OSH).
+template <class TP, int l, int OSH = 0>
 __device__ __forceinline__ void ntt_from(V4* v, uint2* xg, int t, int ql, int bar, const SideTables& tb,
                                          const OddOut& oo, uint64_t col, bool active) {
     using LV = LvlGeom<TP, TP::nlr(l), TP::npre(l)>;
@@ -302,7 +311,7 @@ __device__ __forceinline__ void ntt_from(V4* v, uint2* xg, int t, int ql, int ba
         exchange<TP, LV::R, LV::LOGL, Rd::R, Rd::LOGL>(
             v, xg, ql, bar, [&](int g) { return LV::base(LV::gid(g, t)); },
             [&](int g) { return Rd::base(Rd::gid(g, t)); });
-        ntt_from<TP, l + 1>(v, xg, t, ql, bar, tb, oo, col, active);
+        ntt_from<TP, l + 1, OSH>(v, xg, t, ql, bar, tb, oo, col, active);
     } else {
 #pragma unroll
         for (int g = 0; g < LV::G; g++) dft_dif<TP::nlr(l), false>(v + g * LV::R);
@@ -313,7 +322,8 @@ __device__ __forceinline__ void ntt_from(V4* v, uint2* xg, int t, int ql, int ba
             for (int r = 0; r < LV::R; r++) {
                 const uint32_t k =
                     digit_rev<typename TP::PL, true>((blk << TP::nlr(l)) | (uint32_t)bitrev(r, TP::nlr(l)));
-                if (active && k < oo.rows) stg_stream_v4(oo.p + (uint64_t)k * oo.stride + col, v[g * LV::R + r]);
+                if (active && k < oo.rows && (k & ((1u << OSH) - 1)) == 0)
+                    stg_stream_v4(oo.p + (uint64_t)(k >> OSH) * oo.stride + col, v[g * LV::R + r]);
             }
         }
     }
@@ -365,10 +375,15 @@ __device__ __forceinline__ void stage_read(V4* v, const unsigned char* smem, con
 // (see OddOut).
 // With stagger_pending set, group 0 releases group 1 (named barrier 3) when it
 // starts INTT level stagger_at (NLEV-1: after all INTT levels but the last).
-template <class TP>
+// TWM (the decoder's passes): 0 = the extension's twist (immediates in the last
+// INTT stage); 1 = per-k2 factors ktw[k2] instead; 2 = the same, then the
+// coefficients of the upper half (k2 >= R/2, i.e. index >= S/2) are counted into
+// *cnt where nonzero and set to zero. OSH as in ntt_from.
+template <class TP, int OSH = 0, int TWM = 0>
 __device__ __forceinline__ void tile_compute(V4* v, uint2* xg, const Coords<TP>& c, int bar, const SideTables& tb,
                                              const OddOut& oo, uint64_t col, bool active,
-                                             bool& stagger_pending, int stagger_at = TP::NLEV - 1) {
+                                             bool& stagger_pending, int stagger_at = TP::NLEV - 1,
+                                             const uint2* ktw = nullptr, unsigned long long* cnt = nullptr) {
     const int t = c.t, ql = c.ql;
     // ---- INTT levels 0 .. NLEV-2
     intt_upto_last<TP, 0>(v, xg, t, ql, bar, tb, stagger_pending, stagger_at);
@@ -386,13 +401,23 @@ __device__ __forceinline__ void tile_compute(V4* v, uint2* xg, const Coords<TP>&
         using Rd = LvlGeom<TP, TP::nlr(1), TP::npre(1)>;
 #pragma unroll
         for (int g = 0; g < G; g++) {
-            dft_dif_twout<LR, true, true>(v + g * R, ConstTw<LR + 1, false>{});
+            if constexpr (TWM == 0) dft_dif_twout<LR, true, true>(v + g * R, ConstTw<LR + 1, false>{});
+            else dft_dif_twout<LR, true, true>(v + g * R, KTw{ktw});
             // NTT level 0 wants coefficient c0 + (S/R)*j in register j
             V4 y[R];
 #pragma unroll
             for (int j = 0; j < R; j++) y[j] = v[g * R + bitrev(j, LR)];
 #pragma unroll
             for (int j = 0; j < R; j++) v[g * R + j] = y[j];
+            if constexpr (TWM == 2) {
+#pragma unroll
+                for (int j = R / 2; j < R; j++) {
+                    if (active)
+#pragma unroll
+                        for (int e = 0; e < 4; e++) *cnt += v[g * R + j].c[e] % P != 0;
+                    v[g * R + j] = V4{{0, 0, 0, 0}};
+                }
+            }
             // ---- NTT level 0: radix R over stride S/R, then g^c0/S * omega_S^(c0*k2)
             const TabTw<NB> twf{tb.ntt0 + LV::gid(g, t)};
             dft_dif_twout<LR, false, false>(v + g * R, twf);
@@ -402,7 +427,7 @@ __device__ __forceinline__ void tile_compute(V4* v, uint2* xg, const Coords<TP>&
             [&](int g) { return Rd::base(Rd::gid(g, t)); });
     }
     // ---- NTT levels 1 .. NLEV-1, the last one stores the odd rows
-    ntt_from<TP, 1>(v, xg, t, ql, bar, tb, oo, col, active);
+    ntt_from<TP, 1, OSH>(v, xg, t, ql, bar, tb, oo, col, active);
 }
 
 // Re-derive a value from an opaque copy so the compiler rebuilds per-tile
@@ -484,6 +509,86 @@ __global__ void __launch_bounds__(TPlan<LOG_S, LEPT>::THREADS, 1)
     }
     stagger_release<TP::THREADS>(stagger_pending);
     if (producer) bulk_wait0();
+}
+
+// ---- one pass of the erasure decoder on the TMA-staged shape ---------------------
+// out[r] = NTT_S(mid(i) * INTT_S(pre(j) * in[j])(i))(r) over [S][cols] tiles, with
+// mid(c0 + (S/R) k2) = (block factor of c0, in tb.ntt0) * ktw[k2]: the two
+// passes of zoda_recover_device (general.cu). Rows with pre = 0 are loaded and
+// zeroed (they may hold anything). TWM and OSH as in tile_compute; *counter
+// receives the upper-half count with TWM = 2. Same pipeline as k_extend_tma
+// without the even-row stores.
+template <int LOG_S, int LEPT, int OSH, int TWM>
+__global__ void __launch_bounds__(TPlan<LOG_S, LEPT>::THREADS, 1)
+    k_dec_tma(const __grid_constant__ CUtensorMap tm_in, uint32_t* __restrict__ out, uint64_t out_pitch,
+              uint32_t out_rows, uint64_t cols, uint64_t ntiles, const SideTables tb, const uint2* __restrict__ pre,
+              const uint2* __restrict__ ktw, unsigned long long* __restrict__ counter, int* __restrict__ err,
+              uint32_t flags) {
+    using TP = TPlan<LOG_S, LEPT>;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    uint32_t* stage = reinterpret_cast<uint32_t*>(smem);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + TP::OFF_BAR);
+    uint64_t* empty = full + 1;
+    const int tid = threadIdx.x;
+    const int grp = tid / TP::GS;
+    const int bar = 1 + grp;
+    const bool producer = tid == TP::GS;
+    if (tid == 0) {
+        mbar_init(full, 1);
+        mbar_init(empty, 2);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    const TileRange tr(ntiles, flags & 1);
+    const bool stagger = !(flags & 2);
+    const OddOut oo{out, out_pitch, out_rows};
+    const int stagger_at = (flags >> 2) & 3 ? (int)((flags >> 2) & 3) - 1 : TP::NLEV - 1;
+    unsigned long long cnt = 0;
+    uint64_t tile = tr.first;
+    if (producer && tile < tr.last) tma_load_tile<TP>(stage, &tm_in, tile, full);
+    if (stagger && grp == 1 && tile < tr.last) asm volatile("bar.sync 3, %0;" ::"n"(TP::THREADS) : "memory");
+    bool stagger_pending = stagger && grp == 0 && tile < tr.last;
+    V4 v[TP::EPT];
+    uint32_t parity = 0;
+    for (; tile < tr.last; tile += tr.step, parity ^= 1) {
+        const int tid_l = opaque(tid);
+        const Coords<TP> c(tid_l % TP::GS, grp);
+        uint2* xg = reinterpret_cast<uint2*>(smem + TP::OFF_X + (tid_l / TP::GS) * TP::X_BYTES);
+        const bool ok = mbar_wait_bounded(full, parity);
+        if (group_vote_or(bar, !ok, TP::GS)) {
+            if (tid % TP::GS == 0) atomicOr(err, 1);
+            stagger_release<TP::THREADS>(stagger_pending);
+            return;
+        }
+        const uint64_t col = tile * TP::C + 4 * (uint64_t)c.q;
+        const bool active = col < cols;
+        stage_read<TP>(v, smem, c);
+        group_bar(bar, TP::GS);  // this group has copied the staging buffer out
+        if (tid % TP::GS == 0) mbar_arrive(empty);
+        const uint64_t next = tile + tr.step;
+        if (producer && next < tr.last) {
+            const bool e_ok = mbar_wait_bounded(empty, parity);  // the other group is done too
+            fence_proxy_async();
+            if (e_ok) tma_load_tile<TP>(stage, &tm_in, next, full);
+            else atomicOr(err, 2);  // both groups then time out on `full` and leave
+        }
+        {  // row pre-factors: stage_read gave register j row t + L0*j
+            constexpr int R0 = 1 << TP::lr(0);
+            constexpr int L0 = TP::S / R0;
+#pragma unroll
+            for (int j = 0; j < R0; j++) {
+                const uint2 u = __ldg(pre + (uint32_t)c.t + (uint32_t)L0 * j);
+                mul4(v[j], Tw{u.x, u.y});
+            }
+        }
+        tile_compute<TP, OSH, TWM>(v, xg, c, bar, tb, oo, col, active, stagger_pending, stagger_at, ktw, &cnt);
+    }
+    stagger_release<TP::THREADS>(stagger_pending);
+    if constexpr (TWM == 2) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xFFFFFFFFu, cnt, o);
+        if ((tid & 31) == 0 && cnt) atomicAdd(counter, cnt);
+    }
 }
 
 // ---- many squares of mixed sides in one persistent launch ---------------------------

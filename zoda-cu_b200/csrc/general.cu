@@ -31,6 +31,7 @@
 
 #include "coltx.cuh"
 #include "internal.hpp"
+#include "tma_host.hpp"
 
 namespace zb {
 namespace {
@@ -104,6 +105,110 @@ zoda_status coltx2(const zoda_ctx* ctx, int log_n, bool even_out, const ColTx2& 
         return a.counter ? coltx2_t<L, 1, true>(ctx, a, st) : coltx2_t<L, 1, false>(ctx, a, st);
         ZB_CASE(1) ZB_CASE(2) ZB_CASE(3) ZB_CASE(4) ZB_CASE(5) ZB_CASE(6)
         ZB_CASE(7) ZB_CASE(8) ZB_CASE(9) ZB_CASE(10) ZB_CASE(11) ZB_CASE(12) ZB_CASE(13)
+#undef ZB_CASE
+        default: return ZODA_ERR_UNSUPPORTED;
+    }
+}
+
+// ---- the decoder's passes on the TMA-staged shape (k_dec_tma) ------------------
+// Sides 2^7 .. 2^12 (the TMA-staged range, a whole tile per CTA); level
+// radix 8 from 2048 points, 16 below (as the extension's tuning picks).
+constexpr int DEC_TMA_MIN_LOG = 7, DEC_TMA_MAX_LOG = 12;
+constexpr int dec_lept(int ls) { return ls >= 11 ? 3 : 4; }
+
+// Pattern-independent tables of the two passes for side S = 2^ls, built once:
+//   ntt0_a, ntt0_b  NTT level 0 as in SideTables, with the block factor
+//                   h^(+c0)/S resp. h^(-c0)/S in place of g^c0/S (S entries each)
+//   ktw_a[k2]  = h^((S/R) k2)
+//   ktw_b[k2]  = h^(-(S/R) k2) for k2 < R/2, else 0 (drops coefficients >= S/2)
+//   ktw_bc[k2] = h^(-(S/R) k2) (the checking form zeroes them after counting)
+// so that mid(c0 + (S/R) k2) = block(c0) * ktw[k2] is h^(+-i)/S, resp. that
+// times [i < S/2]. R = 2^lr(last INTT level).
+struct DecTables {
+    const uint2 *ntt0_a, *ntt0_b, *ktw_a, *ktw_b, *ktw_bc;
+};
+zoda_status dec_tables(zoda_ctx* ctx, int ls, DecTables* out) {
+    const int lept = dec_lept(ls);
+    DevBuf& b = ctx->coset_tabs[-1 - ls];  // coset keys are >= 0
+    const int nlev = (ls + lept - 1) / lept;
+    auto lr = [&](int l) { return l < nlev - 1 ? lept : ls - lept * (nlev - 1); };
+    const uint32_t S = 1u << ls;
+    const int LR = lr(nlev - 1);
+    const uint32_t R = 1u << LR, NB = S >> LR, step = S / R;
+    if (!b.p) {
+        std::vector<uint2> h;
+        const uint32_t hinv = powmod_c(GENERATOR, P - 2), sinv = powmod_c(S, P - 2);
+        for (int dir = 0; dir < 2; dir++) {
+            const uint32_t base = dir == 0 ? GENERATOR : hinv;
+            for (uint32_t k2 = 0; k2 < R; k2++)
+                for (uint32_t bb = 0; bb < NB; bb++) {
+                    // c0 = digit reversal of slot bb*R over the INTT radices (as the side tables)
+                    uint32_t slot = bb << LR, c0 = 0;
+                    int sh_in = ls, sh_out = 0;
+                    for (int l = 0; l < nlev; l++) {
+                        sh_in -= lr(l);
+                        c0 |= ((slot >> sh_in) & ((1u << lr(l)) - 1)) << sh_out;
+                        sh_out += lr(l);
+                    }
+                    const uint32_t v = mulmod_c(mulmod_c(powmod_c(base, c0), sinv),
+                                                powmod_c(root_of_unity(ls), (uint64_t)c0 * k2 % S));
+                    h.push_back(shoup_pair(v));
+                }
+        }
+        for (uint32_t k2 = 0; k2 < R; k2++) h.push_back(shoup_pair(powmod_c(GENERATOR, (uint64_t)step * k2)));
+        for (uint32_t k2 = 0; k2 < R; k2++)
+            h.push_back(k2 < R / 2 ? shoup_pair(powmod_c(hinv, (uint64_t)step * k2)) : make_uint2(0u, 0u));
+        for (uint32_t k2 = 0; k2 < R; k2++) h.push_back(shoup_pair(powmod_c(hinv, (uint64_t)step * k2)));
+        zoda_status s = b.ensure(h.size() * sizeof(uint2));
+        if (s != ZODA_OK) return s;
+        ZB_CUDA(cudaMemcpy(b.p, h.data(), h.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+    }
+    const uint2* t = (const uint2*)b.p;
+    *out = DecTables{t, t + S, t + 2 * S, t + 2 * S + R, t + 2 * S + 2 * R};
+    return ZODA_OK;
+}
+
+template <int LS, int OSH, int TWM>
+zoda_status dec_pass_t(const zoda_ctx* ctx, const uint32_t* in, uint64_t in_pitch, const uint2* pre,
+                       const uint2* ntt0, const uint2* ktw, uint32_t* out, uint64_t out_pitch, uint32_t out_rows,
+                       uint64_t w, unsigned long long* counter, cudaStream_t st) {
+    constexpr int LEPT = dec_lept(LS);
+    using TP = TPlan<LS, LEPT>;
+    const uint64_t ntiles = (w + TP::C - 1) / TP::C;
+    if (ntiles == 0) return ZODA_OK;
+    // L2 promotion, tile order and stagger of the side's plan (tuned or default)
+    const zoda_plan p = ctx->planned[LS] ? ctx->plan[LS] : default_plan(LS);
+    const uint32_t at_code = p.stagger == 2 ? 2u : p.stagger == 3 ? 1u : 0u;
+    const uint32_t flags = (p.blocked ? 1u : 0u) | (p.stagger ? 0u : 2u) | (at_code << 2);
+    CUtensorMap m;
+    zoda_status s = make_map(&m, in, w, TP::S, in_pitch * 4, TP::BOX_C, TP::BOX_R, tile_swizzle<TP>(),
+                             p.impl == ZODA_IMPL_TMA ? p.l2_promo : 3);
+    if (s != ZODA_OK) return s;
+    SideTables tb = side_tables(ctx, LS, LEPT);
+    tb.ntt0 = ntt0;
+    ZB_CUDA(cudaFuncSetAttribute(k_dec_tma<LS, LEPT, OSH, TWM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)TP::SMEM));
+    const uint64_t grid = ntiles < (uint64_t)ctx->sm_count ? ntiles : (uint64_t)ctx->sm_count;
+    k_dec_tma<LS, LEPT, OSH, TWM><<<(unsigned)grid, TP::THREADS, TP::SMEM, st>>>(
+        m, out, out_pitch, out_rows, w, ntiles, tb, pre, ktw, counter, ctx->d_err, flags);
+    ZB_CUDA(cudaGetLastError());
+    return ZODA_OK;
+}
+
+// Pass A (second = false) or B of the decoder on side 2^ls, DEC_TMA_MIN_LOG <= ls <= DEC_TMA_MAX_LOG.
+zoda_status dec_pass(const zoda_ctx* ctx, int ls, bool second, const DecTables& t, const uint32_t* in,
+                     uint64_t in_pitch, const uint2* pre, uint32_t* out, uint64_t out_pitch, uint64_t w,
+                     unsigned long long* counter, cudaStream_t st) {
+    const uint32_t S = 1u << ls;
+    switch (ls) {
+#define ZB_CASE(L)                                                                                             \
+    case L:                                                                                                    \
+        if (!second) return dec_pass_t<L, 0, 1>(ctx, in, in_pitch, pre, t.ntt0_a, t.ktw_a, out, out_pitch, S, w, \
+                                                nullptr, st);                                                  \
+        if (counter) return dec_pass_t<L, 1, 2>(ctx, in, in_pitch, pre, t.ntt0_b, t.ktw_bc, out, out_pitch, S, w, \
+                                                counter, st);                                                  \
+        return dec_pass_t<L, 1, 1>(ctx, in, in_pitch, pre, t.ntt0_b, t.ktw_b, out, out_pitch, S, w, nullptr, st);
+        ZB_CASE(7) ZB_CASE(8) ZB_CASE(9) ZB_CASE(10) ZB_CASE(11) ZB_CASE(12)
 #undef ZB_CASE
         default: return ZODA_ERR_UNSUPPORTED;
     }
@@ -372,12 +477,23 @@ zoda_status zoda_recover_device(zoda_ctx* ctx, const uint32_t* d_code, const uin
     const uint64_t w0 = chunk_cols(cols, N);
     if ((s = ctx->gen_a.ensure((uint64_t)N * w0 * 4)) != ZODA_OK) return finish(s);
     uint32_t* A = (uint32_t*)ctx->gen_a.p;
+    const bool tma = ln >= DEC_TMA_MIN_LOG && ln <= DEC_TMA_MAX_LOG;
+    DecTables dt{};
+    if (tma && (s = dec_tables(ctx, ln, &dt)) != ZODA_OK) return finish(s);
     for (uint64_t c0 = 0; c0 < cols; c0 += w0) {
         const uint64_t w = std::min(w0, cols - c0);
+        unsigned long long* cnt = mismatch ? d_cnt : nullptr;
+        if (tma) {  // the same two passes on the TMA-staged shape
+            if ((s = dec_pass(ctx, ln, false, dt, d_code + c0, cols, zk, A, w, w, nullptr, st)) != ZODA_OK)
+                return finish(s);
+            if ((s = dec_pass(ctx, ln, true, dt, A, w, izh, d_data + c0, cols, w, cnt, st)) != ZODA_OK)
+                return finish(s);
+            continue;
+        }
         // pass A: g~ = NTT(h^i / N * INTT(y * Z)) into the scratch
         const ColTx2 pa{d_code + c0, cols, N, zk, (const Tw*)mid_a, A, w, N, w, 0, nullptr};
         // pass B: data row m = even output 2m of NTT(h^-i / N [i < k] * INTT(g~ / Z(h w)))
-        const ColTx2 pb{A, w, N, izh, (const Tw*)mid_b, d_data + c0, cols, N, w, k, mismatch ? d_cnt : nullptr};
+        const ColTx2 pb{A, w, N, izh, (const Tw*)mid_b, d_data + c0, cols, N, w, k, cnt};
         if ((s = coltx2(ctx, ln, false, pa, st)) != ZODA_OK) return finish(s);
         if ((s = coltx2(ctx, ln, true, pb, st)) != ZODA_OK) return finish(s);
     }

@@ -52,12 +52,17 @@ inline zoda_status make_map(CUtensorMap* m, const void* base, uint64_t cols, uin
 // in_rows / even_rows bound the maps (TMA reads zeros past in_rows and clips
 // stores past even_rows); 0 means S.
 template <class TP>
+constexpr CUtensorMapSwizzle tile_swizzle() {
+    return TP::SWZ_MASK == 7   ? CU_TENSOR_MAP_SWIZZLE_128B
+           : TP::SWZ_MASK == 3 ? CU_TENSOR_MAP_SWIZZLE_64B
+           : TP::SWZ_MASK == 1 ? CU_TENSOR_MAP_SWIZZLE_32B
+                               : CU_TENSOR_MAP_SWIZZLE_NONE;
+}
+
+template <class TP>
 zoda_status make_tile_maps(CUtensorMap* m_in, CUtensorMap* m_even, const uint32_t* in, uint32_t* out,
                            uint64_t cols, int promo = 3, uint32_t in_rows = 0, uint32_t even_rows = 0) {
-    const CUtensorMapSwizzle swz = TP::SWZ_MASK == 7   ? CU_TENSOR_MAP_SWIZZLE_128B
-                                   : TP::SWZ_MASK == 3 ? CU_TENSOR_MAP_SWIZZLE_64B
-                                   : TP::SWZ_MASK == 1 ? CU_TENSOR_MAP_SWIZZLE_32B
-                                                       : CU_TENSOR_MAP_SWIZZLE_NONE;
+    const CUtensorMapSwizzle swz = tile_swizzle<TP>();
     zoda_status s = make_map(m_in, in, cols, in_rows ? in_rows : TP::S, cols * 4, TP::BOX_C, TP::BOX_R, swz, promo);
     if (s != ZODA_OK) return s;
     return make_map(m_even, out, cols, even_rows ? even_rows : TP::S, cols * 8, TP::BOX_C, TP::BOX_R, swz);
