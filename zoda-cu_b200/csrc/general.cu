@@ -22,10 +22,12 @@
 // with h = 31 (a generator of F_p^*, never a 2k-th root of unity, so Z(h w) != 0).
 // F~_i must vanish for i >= k when the known rows are one codeword; the
 // optional check counts the entries that do not. The four transforms run as two
-// fused passes (k_coltx2), each an INTT and an NTT with the pointwise factor
-// between them applied in registers: pass A gives g~, pass B gives the data
-// rows as the even outputs of NTT_2k(F~_i * h^-i, zero for i >= k), which is
-// NTT_k of the first k coefficients at omega_2k^(2m) = omega_k^m.
+// fused passes, each an INTT and an NTT with the pointwise factor between them
+// applied in registers: pass A gives g~, pass B gives the data rows as the even
+// outputs of NTT_2k(F~_i * h^-i, zero for i >= k), which is NTT_k of the first
+// k coefficients at omega_2k^(2m) = omega_k^m. From 128 to 4096 points the
+// passes run on the TMA-staged pipeline (k_dec_tma, extend_tma.cuh), elsewhere
+// on the direct-load shape (k_coltx2, coltx.cuh).
 #include <algorithm>
 #include <vector>
 
