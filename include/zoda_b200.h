@@ -141,6 +141,14 @@ void zoda_plan_clear(zoda_ctx* ctx);
  * device first. */
 zoda_status zoda_ctx_check(zoda_ctx* ctx);
 
+/* Self-test of the bounded-wait path every staged kernel uses: one small
+ * kernel waits on a shared-memory barrier that nothing completes. When the
+ * bound runs out (the same 2^18 polls, about a second) it sets the context's
+ * flag and returns, so the next zoda_ctx_check returns ZODA_ERR_TIMEOUT and
+ * clears it; the context stays usable. No counterpart in the reference.
+ * Asynchronous on `stream`. */
+zoda_status zoda_selftest_bounded_wait(zoda_ctx* ctx, void* stream);
+
 /* Fused extension, device memory. d_in is row-major [k][cols], d_out is
  * row-major [2k][cols]; row j of d_out is every column's degree-<k
  * interpolant evaluated at omega_2k^j, i.e. the rows the reference gathers

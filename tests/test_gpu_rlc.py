@@ -20,6 +20,13 @@ def ctx():
     c.close()
 
 
+@pytest.fixture(autouse=True)
+def no_wait_gave_up(ctx):
+    """After every test: no kernel's bounded wait ran out (zoda_ctx_check)."""
+    yield
+    ctx.check()
+
+
 def to_dev(a: np.ndarray):
     return torch.from_numpy(np.ascontiguousarray(a, dtype=np.uint32).view(np.int32)).cuda()
 

@@ -7,6 +7,7 @@
 #include <thread>
 #include <vector>
 
+#include "async.cuh"
 #include "internal.hpp"
 
 namespace zb {
@@ -156,6 +157,17 @@ class EvenRowCopy {
 // Share of the column chunks of a host call whose even output rows return
 // over PCIe rather than through the host copy (measured on B200 hosts).
 constexpr double HOST_EVEN_DEVICE_SHARE = 0.125;
+
+// A wait that nothing completes: the bounded wait gives up and flags it.
+__global__ void k_selftest_wait(int* __restrict__ err) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);  // one arrival expected, none ever made
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (!mbar_wait_bounded(&bar, 0) && threadIdx.x == 0) atomicOr(err, 8);
+}
 
 static int log2_exact(uint64_t x) {
     if (x == 0 || (x & (x - 1))) return -1;
@@ -307,6 +319,14 @@ zoda_status zoda_extend_device(zoda_ctx* ctx, const uint32_t* d_in, uint32_t* d_
 zoda_status zoda_ctx_set_impl(zoda_ctx* ctx, int impl) {
     if (!ctx || impl < 0 || impl > 2) return ZODA_ERR_ARG;
     ctx->impl = impl;
+    return ZODA_OK;
+}
+
+zoda_status zoda_selftest_bounded_wait(zoda_ctx* ctx, void* stream) {
+    if (!ctx) return ZODA_ERR_ARG;
+    ZB_CUDA(cudaSetDevice(ctx->device));
+    k_selftest_wait<<<1, 32, 0, (cudaStream_t)stream>>>(ctx->d_err);
+    ZB_CUDA(cudaGetLastError());
     return ZODA_OK;
 }
 

@@ -27,9 +27,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait: gives up after ~2^22 polls (well over a second) instead of hanging.
+// Bounded wait: gives up after 2^18 polls instead of hanging. A poll that finds
+// the phase incomplete blocks for a few microseconds, so the bound is about a
+// second of the kernel's own running time (measured on B200: 2^22 polls took
+// 17 s); the waits it guards normally end within microseconds.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-    for (uint32_t i = 0; i < (1u << 22); i++)
+    for (uint32_t i = 0; i < (1u << 18); i++)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }

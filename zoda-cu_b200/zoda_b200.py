@@ -32,7 +32,7 @@ STATUS = {
 EXPORTS = [
     "cuda_ntt", "cuda_intt", "cuda_host_alloc", "cuda_host_free",
     "zoda_status_string", "zoda_last_error", "zoda_ctx_create", "zoda_ctx_destroy", "zoda_max_side",
-    "zoda_extend_device", "zoda_extend_host", "zoda_ctx_set_impl", "zoda_ctx_check",
+    "zoda_extend_device", "zoda_extend_host", "zoda_ctx_set_impl", "zoda_ctx_check", "zoda_selftest_bounded_wait",
     "zoda_ntt_device_noalloc", "zoda_batch_create", "zoda_batch_run", "zoda_batch_elements",
     "zoda_batch_destroy", "zoda_server_create", "zoda_server_submit", "zoda_server_wait",
     "zoda_server_release", "zoda_server_cancel", "zoda_server_get_stats", "zoda_server_destroy",
@@ -127,6 +127,8 @@ def load(path: str = LIB_PATH):
     L.zoda_ctx_set_impl.argtypes = [vp, ctypes.c_int]
     L.zoda_ctx_check.restype = ctypes.c_int
     L.zoda_ctx_check.argtypes = [vp]
+    L.zoda_selftest_bounded_wait.restype = ctypes.c_int
+    L.zoda_selftest_bounded_wait.argtypes = [vp, vp]
     L.zoda_batch_create.restype = ctypes.c_int
     L.zoda_batch_create.argtypes = [vp, ctypes.POINTER(ZodaSquare), ctypes.c_uint32, ctypes.POINTER(vp)]
     L.zoda_batch_run.restype = ctypes.c_int
@@ -321,6 +323,11 @@ class Context:
     def check(self):
         """Raise if a kernel on this context gave up a bounded wait (synchronizes)."""
         _check(load().zoda_ctx_check(self._h), "zoda_ctx_check")
+
+    def selftest_bounded_wait(self, stream=None):
+        """Run a kernel whose barrier wait nothing completes; the next check() raises
+        ZODA_ERR_TIMEOUT (and clears the flag)."""
+        _check(load().zoda_selftest_bounded_wait(self._h, _stream_handle(stream)), "zoda_selftest_bounded_wait")
 
     def extend_host(self, h_in, h_out, k: int, cols: int) -> ZodaTiming:
         t = ZodaTiming()
