@@ -61,6 +61,13 @@ SHAPES = [
     (300, 212),   # n_k 512, fused, n_kn 1024 exactly filled
     (1500, 1000), # n_k 2048, fused with the tuned side-2048 plan
     (3000, 3000), # n_k 4096, fused (direct kernel)
+    # n_kn >= 4 n_k with n_k 128 .. 2048: one fused TMA-staged pass per coset
+    (100, 300),   # n_k 128, R = 4
+    (129, 900),   # n_k 256 (k just past a power of two), n_kn 2048: R = 8
+    (200, 1800),  # n_k 256, R = 8
+    (500, 7500),  # n_k 512, R = 16
+    (1000, 3000), # n_k 1024, R = 4
+    (2000, 6000), # n_k 2048, R = 4
 ]
 
 

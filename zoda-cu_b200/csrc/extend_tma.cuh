@@ -515,10 +515,11 @@ __global__ void __launch_bounds__(TPlan<LOG_S, LEPT>::THREADS, 1)
 // out[r] = NTT_S(mid(i) * INTT_S(pre(j) * in[j])(i))(r) over [S][cols] tiles, with
 // mid(c0 + (S/R) k2) = (block factor of c0, in tb.ntt0) * ktw[k2]: the two
 // passes of zoda_recover_device (general.cu). Rows with pre = 0 are loaded and
-// zeroed (they may hold anything). TWM and OSH as in tile_compute; *counter
-// receives the upper-half count with TWM = 2. Same pipeline as k_extend_tma
-// without the even-row stores.
-template <int LOG_S, int LEPT, int OSH, int TWM>
+// zeroed (they may hold anything); with PRE = false there are no pre-factors
+// (the any-shape encode's coset passes). TWM and OSH as in tile_compute;
+// *counter receives the upper-half count with TWM = 2. Same pipeline as
+// k_extend_tma without the even-row stores.
+template <int LOG_S, int LEPT, int OSH, int TWM, bool PRE = true>
 __global__ void __launch_bounds__(TPlan<LOG_S, LEPT>::THREADS, 1)
     k_dec_tma(const __grid_constant__ CUtensorMap tm_in, uint32_t* __restrict__ out, uint64_t out_pitch,
               uint32_t out_rows, uint64_t cols, uint64_t ntiles, const SideTables tb, const uint2* __restrict__ pre,
@@ -572,7 +573,7 @@ __global__ void __launch_bounds__(TPlan<LOG_S, LEPT>::THREADS, 1)
             if (e_ok) tma_load_tile<TP>(stage, &tm_in, next, full);
             else atomicOr(err, 2);  // both groups then time out on `full` and leave
         }
-        {  // row pre-factors: stage_read gave register j row t + L0*j
+        if constexpr (PRE) {  // row pre-factors: stage_read gave register j row t + L0*j
             constexpr int R0 = 1 << TP::lr(0);
             constexpr int L0 = TP::S / R0;
 #pragma unroll

@@ -170,10 +170,11 @@ zoda_status dec_tables(zoda_ctx* ctx, int ls, DecTables* out) {
     return ZODA_OK;
 }
 
-template <int LS, int OSH, int TWM>
+// One k_dec_tma launch over w columns; input rows >= in_rows (0: S) read as zeros.
+template <int LS, int OSH, int TWM, bool PRE = true>
 zoda_status dec_pass_t(const zoda_ctx* ctx, const uint32_t* in, uint64_t in_pitch, const uint2* pre,
                        const uint2* ntt0, const uint2* ktw, uint32_t* out, uint64_t out_pitch, uint32_t out_rows,
-                       uint64_t w, unsigned long long* counter, cudaStream_t st) {
+                       uint64_t w, unsigned long long* counter, cudaStream_t st, uint32_t in_rows = 0) {
     constexpr int LEPT = dec_lept(LS);
     using TP = TPlan<LS, LEPT>;
     const uint64_t ntiles = (w + TP::C - 1) / TP::C;
@@ -183,15 +184,15 @@ zoda_status dec_pass_t(const zoda_ctx* ctx, const uint32_t* in, uint64_t in_pitc
     const uint32_t at_code = p.stagger == 2 ? 2u : p.stagger == 3 ? 1u : 0u;
     const uint32_t flags = (p.blocked ? 1u : 0u) | (p.stagger ? 0u : 2u) | (at_code << 2);
     CUtensorMap m;
-    zoda_status s = make_map(&m, in, w, TP::S, in_pitch * 4, TP::BOX_C, TP::BOX_R, tile_swizzle<TP>(),
-                             p.impl == ZODA_IMPL_TMA ? p.l2_promo : 3);
+    zoda_status s = make_map(&m, in, w, in_rows ? in_rows : TP::S, in_pitch * 4, TP::BOX_C, TP::BOX_R,
+                             tile_swizzle<TP>(), p.impl == ZODA_IMPL_TMA ? p.l2_promo : 3);
     if (s != ZODA_OK) return s;
     SideTables tb = side_tables(ctx, LS, LEPT);
     tb.ntt0 = ntt0;
-    ZB_CUDA(cudaFuncSetAttribute(k_dec_tma<LS, LEPT, OSH, TWM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)TP::SMEM));
+    ZB_CUDA(cudaFuncSetAttribute(k_dec_tma<LS, LEPT, OSH, TWM, PRE>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TP::SMEM));
     const uint64_t grid = ntiles < (uint64_t)ctx->sm_count ? ntiles : (uint64_t)ctx->sm_count;
-    k_dec_tma<LS, LEPT, OSH, TWM><<<(unsigned)grid, TP::THREADS, TP::SMEM, st>>>(
+    k_dec_tma<LS, LEPT, OSH, TWM, PRE><<<(unsigned)grid, TP::THREADS, TP::SMEM, st>>>(
         m, out, out_pitch, out_rows, w, ntiles, tb, pre, ktw, counter, ctx->d_err, flags);
     ZB_CUDA(cudaGetLastError());
     return ZODA_OK;
@@ -210,6 +211,74 @@ zoda_status dec_pass(const zoda_ctx* ctx, int ls, bool second, const DecTables& 
         if (counter) return dec_pass_t<L, 1, 2>(ctx, in, in_pitch, pre, t.ntt0_b, t.ktw_bc, out, out_pitch, S, w, \
                                                 counter, st);                                                  \
         return dec_pass_t<L, 1, 1>(ctx, in, in_pitch, pre, t.ntt0_b, t.ktw_b, out, out_pitch, S, w, nullptr, st);
+        ZB_CASE(7) ZB_CASE(8) ZB_CASE(9) ZB_CASE(10) ZB_CASE(11) ZB_CASE(12)
+#undef ZB_CASE
+        default: return ZODA_ERR_UNSUPPORTED;
+    }
+}
+
+// Coset passes of the any-shape encode on the TMA-staged shape, for n_k = 2^lp
+// in the decoder's TMA range: coset c of n_kn = 2^ln is
+//   NTT_{n_k}(omega_{n_kn}^(c i) / n_k * INTT_{n_k}(data))
+// in one pass (k_dec_tma without pre-factors; rows >= k arrive as zeros). The
+// twist splits as the extension's does: block factor omega_{n_kn}^(c c0) / n_k
+// in NTT level 0's table, digit factor omega_{n_kn}^(c (S/R) k2) in the INTT's
+// last stage. Tables for every coset c in [1, R), built once per shape:
+// coset c's [ntt0 (S entries) | ktw (R entries)] at (c - 1) * (S + R).
+zoda_status enc_tables(zoda_ctx* ctx, int lp, int ln, const uint2** out, uint32_t* stride) {
+    const int lept = dec_lept(lp);
+    DevBuf& b = ctx->coset_tabs[-(100000 + lp * 64 + ln)];  // disjoint from the other keys
+    const int nlev = (lp + lept - 1) / lept;
+    auto lr = [&](int l) { return l < nlev - 1 ? lept : lp - lept * (nlev - 1); };
+    const uint32_t S = 1u << lp;
+    const int LR = lr(nlev - 1);
+    const uint32_t R = 1u << LR, NB = S >> LR, step = S / R;
+    const uint64_t cosets = (1ull << (ln - lp)) - 1;
+    if (!b.p) {
+        // c0 of every INTT last-level block (digit reversal of slot bb*R), and
+        // omega_S^e: each entry is then two products
+        std::vector<uint32_t> c0s(NB), ws(S);
+        for (uint32_t bb = 0; bb < NB; bb++) {
+            uint32_t slot = bb << LR, c0 = 0;
+            int sh_in = lp, sh_out = 0;
+            for (int l = 0; l < nlev; l++) {
+                sh_in -= lr(l);
+                c0 |= ((slot >> sh_in) & ((1u << lr(l)) - 1)) << sh_out;
+                sh_out += lr(l);
+            }
+            c0s[bb] = c0;
+        }
+        const uint32_t wS = root_of_unity(lp);
+        for (uint32_t e = 0, x = 1; e < S; e++, x = mulmod_c(x, wS)) ws[e] = x;
+        std::vector<uint2> h;
+        h.reserve(cosets * (S + R));
+        std::vector<uint32_t> pw(NB);  // base^i / S for i < NB (every c0 is below S / R = NB)
+        const uint32_t sinv = powmod_c(S, P - 2), wn = root_of_unity(ln);
+        for (uint64_t c = 1, base = wn; c <= cosets; c++, base = mulmod_c((uint32_t)base, wn)) {
+            for (uint32_t i = 0, x = sinv; i < NB; i++, x = mulmod_c(x, (uint32_t)base)) pw[i] = x;
+            for (uint32_t k2 = 0; k2 < R; k2++)
+                for (uint32_t bb = 0; bb < NB; bb++)
+                    h.push_back(shoup_pair(mulmod_c(pw[c0s[bb]], ws[(uint64_t)c0s[bb] * k2 % S])));
+            const uint32_t g = powmod_c((uint32_t)base, step);
+            for (uint32_t k2 = 0, x = 1; k2 < R; k2++, x = mulmod_c(x, g)) h.push_back(shoup_pair(x));
+        }
+        zoda_status s = b.ensure(h.size() * sizeof(uint2));
+        if (s != ZODA_OK) return s;
+        ZB_CUDA(cudaMemcpy(b.p, h.data(), h.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+    }
+    *out = (const uint2*)b.p;
+    *stride = S + R;
+    return ZODA_OK;
+}
+
+// Coset c's pass: output rows R*m + c (m < mc) of out, pitch out_pitch.
+zoda_status enc_coset_pass(const zoda_ctx* ctx, int lp, const uint2* tab, const uint32_t* in, uint32_t k,
+                           uint64_t cols, uint32_t* out, uint64_t out_pitch, uint32_t mc, cudaStream_t st) {
+    const uint2* ntt0 = tab;
+    const uint2* ktw = tab + (1u << lp);
+    switch (lp) {
+#define ZB_CASE(L) \
+    case L: return dec_pass_t<L, 0, 1, false>(ctx, in, cols, nullptr, ntt0, ktw, out, out_pitch, mc, cols, nullptr, st, k);
         ZB_CASE(7) ZB_CASE(8) ZB_CASE(9) ZB_CASE(10) ZB_CASE(11) ZB_CASE(12)
 #undef ZB_CASE
         default: return ZODA_ERR_UNSUPPORTED;
@@ -341,9 +410,21 @@ zoda_status encode_general(zoda_ctx* ctx, const uint32_t* in, uint32_t* out, uin
         }
         return ZODA_OK;
     }
+    zoda_status s;
+    if (lp >= DEC_TMA_MIN_LOG && lp <= DEC_TMA_MAX_LOG) {  // one fused TMA-staged pass per coset, no scratch
+        const uint2* et = nullptr;
+        uint32_t es = 0;
+        if ((s = enc_tables(ctx, lp, ln, &et, &es)) != ZODA_OK) return s;
+        for (uint64_t c = 1; c < R && c < rows_out; c++) {
+            const uint32_t mc = (uint32_t)std::min<uint64_t>(P_, (rows_out - c + R - 1) / R);
+            if ((s = enc_coset_pass(ctx, lp, et + (c - 1) * es, in, k, cols, out + c * cols, R * cols, mc, st)) !=
+                ZODA_OK)
+                return s;
+        }
+        return ZODA_OK;
+    }
     const uint2* tabs = nullptr;
-    zoda_status s = coset_table(ctx, lp, ln, &tabs);
-    if (s != ZODA_OK) return s;
+    if ((s = coset_table(ctx, lp, ln, &tabs)) != ZODA_OK) return s;
     const uint64_t w0 = chunk_cols(cols, P_);
     if ((s = ctx->gen_a.ensure(P_ * w0 * 4)) != ZODA_OK) return s;
     uint32_t* A = (uint32_t*)ctx->gen_a.p;
