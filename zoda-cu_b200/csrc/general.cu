@@ -9,8 +9,10 @@
 //   c = 0:  the padded data row m (a copy),
 //   c > 0:  NTT_{n_k}(omega_{n_kn}^(c*i) * coef_i)[m], one transform per coset.
 // R = 2 (every square, and any n <= 2 n_k - k) runs on the fused extension
-// kernels, which read zeros past row k and stop writing after row k+n; the
-// other shapes take the interpolation + per-coset evaluation path below.
+// kernels, which read zeros past row k and stop writing after row k+n. For
+// R >= 4 with 128 <= n_k <= 4096 each coset c is one fused TMA-staged pass
+// NTT(omega_{n_kn}^(c i) / n_k * INTT(data)) (enc_coset_pass); other n_k take
+// one interpolation and a per-coset evaluation on the direct-load shape.
 //
 // Decoder: f of degree < k is known at a set K of the 2k points omega_2k^j.
 // With Z(x) = prod over the erased points of (x - omega^e), g = f * Z has
