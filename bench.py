@@ -322,8 +322,12 @@ def time_encode_general(ctx, k: int, n: int, reps: int = 5) -> dict:
     ok = bool(torch.equal(d_out[0::r][:m, :256], d_in[:m, :256]))
     del d_in, d_out
     torch.cuda.empty_cache()
-    api = ("zoda_encode_device (n_kn = 2 n_k: the fused kernels, zeros past row k, output cut at k+n)" if r == 2 else
-           f"zoda_encode_device (n_kn = {r} n_k: one interpolation over n_k, {r - 1} coset evaluations)")
+    if r == 2:
+        api = "zoda_encode_device (n_kn = 2 n_k: the fused kernels, zeros past row k, output cut at k+n)"
+    elif 128 <= n_k <= 4096:
+        api = f"zoda_encode_device (n_kn = {r} n_k: one fused TMA-staged INTT + NTT pass per coset, {r - 1} passes)"
+    else:
+        api = f"zoda_encode_device (n_kn = {r} n_k: one interpolation over n_k, {r - 1} coset evaluations)"
     return {"k": k, "n": n, "cols": cols, "ms": round(ms, 4),
             "gbps": round(k * k * 512 * 8.0 / (ms * 1e-3) / 1e9, 1), "data_rows_ok": ok, "api": api}
 
