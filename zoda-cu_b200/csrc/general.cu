@@ -115,10 +115,12 @@ zoda_status coltx2(const zoda_ctx* ctx, int log_n, bool even_out, const ColTx2& 
 }
 
 // ---- the decoder's passes on the TMA-staged shape (k_dec_tma) ------------------
-// Sides 2^7 .. 2^12 (the TMA-staged range, a whole tile per CTA); level
-// radix 8 from 2048 points, 16 below (as the extension's tuning picks).
+// Sides 2^7 .. 2^12 (the TMA-staged range, a whole tile per CTA). Level radix
+// 8 at 512 and 2048 points, 16 at the others: the faster shape of each for the
+// decoder on B200 (interleaved runs on one box: 3-4% apart at 512 and 4096
+// points, equal at 1024 and 2048).
 constexpr int DEC_TMA_MIN_LOG = 7, DEC_TMA_MAX_LOG = 12;
-constexpr int dec_lept(int ls) { return ls >= 11 ? 3 : 4; }
+constexpr int dec_lept(int ls) { return ls == 9 || ls == 11 ? 3 : 4; }
 
 // Pattern-independent tables of the two passes for side S = 2^ls, built once:
 //   ntt0_a, ntt0_b  NTT level 0 as in SideTables, with the block factor
