@@ -99,16 +99,10 @@ static void build_side_tables(int ls, int lept, std::vector<Tw>& all, size_t off
         const uint32_t NB = S >> LR;
         const uint32_t g = root_of_unity(ls + 1);
         const uint32_t s_inv = powmod_c(S, P - 2);
+        const std::vector<uint32_t> c0s = SideLevels(ls, lept).last_c0();
         for (int k2 = 0; k2 < R; k2++)
             for (uint32_t b = 0; b < NB; b++) {
-                // c0 = digit reversal of slot b*R over the INTT radices
-                uint32_t slot = b << LR, c0 = 0;
-                int sh_in = ls, sh_out = 0;
-                for (int l = 0; l < nlev; l++) {
-                    sh_in -= lr(l);
-                    c0 |= ((slot >> sh_in) & ((1u << lr(l)) - 1)) << sh_out;
-                    sh_out += lr(l);
-                }
+                const uint32_t c0 = c0s[b];
                 const uint32_t v = mulmod_c(mulmod_c(powmod_c(g, c0), s_inv), pow_root(ls, (uint64_t)c0 * k2 % S));
                 all.push_back(tw_of(v));
             }

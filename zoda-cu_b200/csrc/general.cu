@@ -134,28 +134,20 @@ struct DecTables {
     const uint2 *ntt0_a, *ntt0_b, *ktw_a, *ktw_b, *ktw_bc;
 };
 zoda_status dec_tables(zoda_ctx* ctx, int ls, DecTables* out) {
-    const int lept = dec_lept(ls);
+    const SideLevels sl(ls, dec_lept(ls));
     DevBuf& b = ctx->coset_tabs[-1 - ls];  // coset keys are >= 0
-    const int nlev = (ls + lept - 1) / lept;
-    auto lr = [&](int l) { return l < nlev - 1 ? lept : ls - lept * (nlev - 1); };
     const uint32_t S = 1u << ls;
-    const int LR = lr(nlev - 1);
+    const int LR = sl.last_lr();
     const uint32_t R = 1u << LR, NB = S >> LR, step = S / R;
     if (!b.p) {
         std::vector<uint2> h;
         const uint32_t hinv = powmod_c(GENERATOR, P - 2), sinv = powmod_c(S, P - 2);
+        const std::vector<uint32_t> c0s = sl.last_c0();
         for (int dir = 0; dir < 2; dir++) {
             const uint32_t base = dir == 0 ? GENERATOR : hinv;
             for (uint32_t k2 = 0; k2 < R; k2++)
                 for (uint32_t bb = 0; bb < NB; bb++) {
-                    // c0 = digit reversal of slot bb*R over the INTT radices (as the side tables)
-                    uint32_t slot = bb << LR, c0 = 0;
-                    int sh_in = ls, sh_out = 0;
-                    for (int l = 0; l < nlev; l++) {
-                        sh_in -= lr(l);
-                        c0 |= ((slot >> sh_in) & ((1u << lr(l)) - 1)) << sh_out;
-                        sh_out += lr(l);
-                    }
+                    const uint32_t c0 = c0s[bb];
                     const uint32_t v = mulmod_c(mulmod_c(powmod_c(base, c0), sinv),
                                                 powmod_c(root_of_unity(ls), (uint64_t)c0 * k2 % S));
                     h.push_back(shoup_pair(v));
@@ -230,28 +222,16 @@ zoda_status dec_pass(const zoda_ctx* ctx, int ls, bool second, const DecTables& 
 // last stage. Tables for every coset c in [1, R), built once per shape:
 // coset c's [ntt0 (S entries) | ktw (R entries)] at (c - 1) * (S + R).
 zoda_status enc_tables(zoda_ctx* ctx, int lp, int ln, const uint2** out, uint32_t* stride) {
-    const int lept = dec_lept(lp);
+    const SideLevels sl(lp, dec_lept(lp));
     DevBuf& b = ctx->coset_tabs[-(100000 + lp * 64 + ln)];  // disjoint from the other keys
-    const int nlev = (lp + lept - 1) / lept;
-    auto lr = [&](int l) { return l < nlev - 1 ? lept : lp - lept * (nlev - 1); };
     const uint32_t S = 1u << lp;
-    const int LR = lr(nlev - 1);
+    const int LR = sl.last_lr();
     const uint32_t R = 1u << LR, NB = S >> LR, step = S / R;
     const uint64_t cosets = (1ull << (ln - lp)) - 1;
     if (!b.p) {
-        // c0 of every INTT last-level block (digit reversal of slot bb*R), and
-        // omega_S^e: each entry is then two products
-        std::vector<uint32_t> c0s(NB), ws(S);
-        for (uint32_t bb = 0; bb < NB; bb++) {
-            uint32_t slot = bb << LR, c0 = 0;
-            int sh_in = lp, sh_out = 0;
-            for (int l = 0; l < nlev; l++) {
-                sh_in -= lr(l);
-                c0 |= ((slot >> sh_in) & ((1u << lr(l)) - 1)) << sh_out;
-                sh_out += lr(l);
-            }
-            c0s[bb] = c0;
-        }
+        // c0 of every INTT last-level block, and omega_S^e: each entry is then two products
+        const std::vector<uint32_t> c0s = sl.last_c0();
+        std::vector<uint32_t> ws(S);
         const uint32_t wS = root_of_unity(lp);
         for (uint32_t e = 0, x = 1; e < S; e++, x = mulmod_c(x, wS)) ws[e] = x;
         std::vector<uint2> h;

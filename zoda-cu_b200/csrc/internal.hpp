@@ -6,6 +6,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/zoda_b200.h"
 #include "field.cuh"
@@ -24,6 +25,33 @@ void set_last_error_text(const std::string& s);
             return ZODA_ERR_CUDA;                    \
         }                                            \
     } while (0)
+
+// Level structure of the TMA kernels' side 2^ls with level radix 2^lept
+// (ExtPlan with schedule 0): full levels of lept bits, the leftover last.
+struct SideLevels {
+    int nlev, lept, ls;
+    SideLevels(int ls_, int lept_) : nlev((ls_ + lept_ - 1) / lept_), lept(lept_), ls(ls_) {}
+    int lr(int l) const { return l < nlev - 1 ? lept : ls - lept * (nlev - 1); }
+    int last_lr() const { return lr(nlev - 1); }
+    // c0 of INTT last-level block b: the digit reversal of slot b * R over the
+    // INTT radices, the first coefficient index the block holds
+    std::vector<uint32_t> last_c0() const {
+        const int LR = last_lr();
+        const uint32_t NB = (1u << ls) >> LR;
+        std::vector<uint32_t> c0s(NB);
+        for (uint32_t b = 0; b < NB; b++) {
+            uint32_t slot = b << LR, c0 = 0;
+            int sh_in = ls, sh_out = 0;
+            for (int l = 0; l < nlev; l++) {
+                sh_in -= lr(l);
+                c0 |= ((slot >> sh_in) & ((1u << lr(l)) - 1)) << sh_out;
+                sh_out += lr(l);
+            }
+            c0s[b] = c0;
+        }
+        return c0s;
+    }
+};
 
 // Grow-only device buffer owned by a context.
 struct DevBuf {
