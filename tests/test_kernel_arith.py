@@ -1,7 +1,9 @@
 """CPU restatements of the arithmetic the device kernels rely on, checked with
 exact Python integers: the RLC kernels' centered residues, signed 64-bit sums
-and folds (csrc/rlc.cu), and the identities behind the decoder's two fused
-passes (csrc/general.cu, k_coltx2 in csrc/coltx.cuh). No GPU needed."""
+and folds (csrc/rlc.cu), the identities behind the decoder's two fused passes
+(csrc/general.cu, k_coltx2 in csrc/coltx.cuh), and the split of the TMA-staged
+passes' middle factor into block and digit tables (k_dec_tma in
+csrc/extend_tma.cuh, the tables in csrc/general.cu). No GPU needed."""
 import numpy as np
 import pytest
 
@@ -186,3 +188,50 @@ def test_decoder_check_catches_a_corrupted_row(k):
     assert high > 0
     _, high_ok = decoder_fused_passes(code[:, 0], known, k)
     assert high_ok == 0
+
+
+# ---- the TMA-staged passes' factor split --------------------------------------------
+
+def last_c0(ls: int, lept: int):
+    """c0 of every INTT last-level block (SideLevels::last_c0 in internal.hpp)."""
+    nlev = (ls + lept - 1) // lept
+    lr = lambda l: lept if l < nlev - 1 else ls - lept * (nlev - 1)
+    LR = lr(nlev - 1)
+    out = []
+    for b in range((1 << ls) >> LR):
+        slot, c0, sh_in, sh_out = b << LR, 0, ls, 0
+        for l in range(nlev):
+            sh_in -= lr(l)
+            c0 |= ((slot >> sh_in) & ((1 << lr(l)) - 1)) << sh_out
+            sh_out += lr(l)
+        out.append(c0)
+    return out, 1 << LR
+
+
+def dec_lept(ls: int) -> int:  # the radix rule of general.cu
+    return 3 if ls in (9, 11) else 4
+
+
+@pytest.mark.parametrize("ls", [7, 8, 9, 10, 11, 12])
+def test_middle_factor_splits_into_block_and_digit_parts(ls):
+    """mid(c0 + (S/R) k2) = block(c0) * digit(k2) for the decoder's two passes and
+    for an encode coset, over every coefficient index exactly once."""
+    S = 1 << ls
+    c0s, R = last_c0(ls, dec_lept(ls))
+    step = S // R
+    idx = sorted(c0 + step * k2 for c0 in c0s for k2 in range(R))
+    assert idx == list(range(S)) and max(c0s) < S // R
+    sinv = modpow(S, P - 2)
+    h, hinv = 31, modpow(31, P - 2)
+    w = int(O.roots_of_unity(4 * S)[1])  # coset c = 1 of n_kn = 4 n_k
+    for c0 in c0s[:: max(1, len(c0s) // 64)]:
+        for k2 in range(R):
+            i = c0 + step * k2
+            # pass A: h^i / S
+            assert modpow(h, c0) * sinv * modpow(h, step * k2) % P == modpow(h, i) * sinv % P
+            # pass B: h^-i / S for i < S/2, else 0 (the digit factor is 0 for k2 >= R/2)
+            digit_b = modpow(hinv, step * k2) if k2 < R // 2 else 0
+            want_b = modpow(hinv, i) * sinv % P if i < S // 2 else 0
+            assert modpow(hinv, c0) * sinv * digit_b % P == want_b
+            # encode coset: omega_{4S}^i / S
+            assert modpow(w, c0) * sinv * modpow(w, step * k2) % P == modpow(w, i) * sinv % P
