@@ -156,23 +156,24 @@ def barrier(world: int):
 # CPU baseline: the reference's CPU path restated (oracle/zoda_oracle.c)
 # ---------------------------------------------------------------------------
 
-def cpu_port_rate(side: int, budget_s: float, seed: int = 1) -> dict:
+def cpu_port_rate(side: int, budget_s: float, seed: int = 1, threads: int = 0) -> dict:
     """Gb/s of the oracle port on a bounded column sample of the side x side square
-    (columns are independent, so a sample of them costs its share of the full square)."""
+    (columns are independent, so a sample of them costs its share of the full square),
+    on `threads` host threads (0: all of them)."""
     import oracle as O
     cols = side * SHARE_U32
-    threads = O.num_threads()
+    threads = threads or O.num_threads()
     # calibrate on a small window, then size the sample to the budget
     probe = max(4, min(cols, 16 * threads))
     src = O.seeded_input(side, probe, seed=seed)
     t0 = time.perf_counter()
-    O.encode_rowmajor(src)
+    O.encode_rowmajor(src, threads=threads)
     dt = time.perf_counter() - t0
     ncols = int(min(cols, max(probe, probe * budget_s / max(dt, 1e-6))))
     ncols -= ncols % 4
     src = O.seeded_input(side, ncols, seed=seed)
     t0 = time.perf_counter()
-    O.encode_rowmajor(src)
+    O.encode_rowmajor(src, threads=threads)
     dt = time.perf_counter() - t0
     frac = ncols / cols
     gbps = payload_bits(side) * frac / dt / 1e9
@@ -619,6 +620,10 @@ def run_ours(args, world, rank, local):
     if rank == 0 and world == 1:
         cpu = cpu_port_rate(side, args.cpu_budget)
         cpu.pop("seconds", None)
+        if not args.no_extra:  # the port on one thread, as the reference's CPU path runs
+            one = cpu_port_rate(side, max(2.0, args.cpu_budget / 4), threads=1)
+            one.pop("seconds", None)
+            extra["cpu_port_single_thread"] = one
     if world > 1:
         barrier(world)
     if rank == 0:
