@@ -1,12 +1,16 @@
 #!/usr/bin/env python3
 """Benchmark of the fused ZODA column extension on B200.
 
-One step = one fused extension of a full data square that is already
-resident in HBM: row-major [side][side*128] u32 BabyBear (512-byte shares)
--> row-major [2*side][side*128]. The default workload is the 1024x1024 square
-(512 MiB in, 1 GiB out, both far larger than the 126 MB L2, so no flush is
-needed between steps). Metric: payload Gb/s = side^2 * 512 * 8 / t / 1e9, the
-reference's definition (src/benchmarks/celestia_squares.rs:71-85).
+One step = one extension of a full data square that is already resident in
+HBM: row-major [side][side*128] u32 BabyBear (512-byte shares) -> row-major
+[2*side][side*128]. The default workload is the 4096x4096 square, the largest
+configuration that fits one GPU (8 GiB in, 16 GiB out, both far larger than
+the 126 MB L2, so no flush is needed between steps); the 1024 and 2048 squares
+are reported beside it with the same fields. Metric: payload Gb/s =
+side^2 * 512 * 8 / t / 1e9, the reference's definition
+(src/benchmarks/celestia_squares.rs:71-85). The output of the last timed step
+is checked in full: the RLC check of every encoded row on the device, with
+coefficients from the SHA-256 data root of the encoded rows.
 
 Lines printed by rank 0 (one JSON object):
   --impl ours       (default) the CUDA library through its C ABI
@@ -200,9 +204,7 @@ def run_reference(args, world, rank):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Gb/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_step, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded uniform in [0,p))",
-        "config": {"workload": f"plain extension of one {side}x{side} square ([{side}][{side * SHARE_U32}] u32 -> "
-                               f"[{2 * side}][{side * SHARE_U32}]), CPU path", "side": side,
-                   "cols": side * SHARE_U32, "l2": "n/a (host)"},
+        "config": workload_config(side),
         "cpu_baseline": {"value": value, "unit": "Gb/s", "cores": last["cores"], "kind": "port",
                          "sample": last["sample"] + "; ms_per_step extrapolated to the full square"},
         "e2e": {"value": value, "unit": "Gb/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -227,6 +229,95 @@ def kernel_name(side: int, plan: dict | None = None) -> str:
 def tune(ctx, side: int, cols: int, reps: int = 3) -> dict:
     """Autotune one side at the workload's own column count (zoda_autotune) and return the plan it installed."""
     return ctx.autotune(side, side, cols, reps)[side]
+
+
+def time_extend_leg(ctx, side: int, cols: int, steps: int, warmup: int) -> dict:
+    """`steps` timed extensions of a [side][cols] slab (a small case of the full square's kernel, for
+    profiling), its output checked in full."""
+    ms, _, check = time_device_extend(ctx, side, steps, warmup, 1, cols=cols)
+    t = ms / steps
+    return {"side": side, "cols": cols, "ms_per_step": round(t, 4),
+            "ps_per_element": round(t * 1e9 / (side * cols), 3),
+            "hbm_frac": round(12.0 * side * cols / (t * 1e-3) / 1e9 / measured_peaks()["hbm_gbs"], 4),
+            "check_mismatches": check["check_mismatches"], "even_rows_equal_data": check["even_rows_equal_data"]}
+
+
+def footprint_sweep(ctx, side: int, reps: int = 5) -> list:
+    """Time per element of the side's extension against its footprint (input + output bytes): the same
+    kernel and tiles on 1/32 .. all of the square's columns. A time per element that grows with the
+    footprint at a fixed per-element work points at address translation, not arithmetic or bandwidth."""
+    import torch
+    full = side * SHARE_U32
+    out = []
+    for div in (32, 16, 8, 4, 2, 1):
+        cols = full // div
+        ms, _, _ = time_device_extend(ctx, side, reps, 2, 1, verify=False, cols=cols)
+        t = ms / reps
+        out.append({"cols": cols, "footprint_gb": round(12.0 * side * cols / 1e9, 2), "ms": round(t, 4),
+                    "ps_per_element": round(t * 1e9 / (side * cols), 3)})
+        torch.cuda.empty_cache()
+    return out
+
+
+def time_long_leg(ctx) -> dict:
+    """The long-column (four-step) path: the reference's validated configurations (k = n = 32768
+    and 65536 on 1024 columns, src/benchmarks/zoda_validated.rs:105-126) device-resident; a
+    131072-point cuda_ntt on host buffers beside the reference's own CUDA kernel on the same
+    call; and the four-step plan at the full 4096 square in each launch shape."""
+    import ctypes
+    import numpy as np
+    import torch
+    import zoda_b200
+    out = {}
+    for k in (32768, 65536):
+        cols = 1024
+        ms, _, check = time_device_extend(ctx, k, 5, 3, 1, cols=cols)
+        t = ms / 5
+        out[f"encode_k{k}_cols{cols}"] = {
+            "ms": round(t, 4), "payload_gbps": round(k * cols * 4 * 8 / (t * 1e-3) / 1e9, 1),
+            "hbm_frac_of_12B": round(12.0 * k * cols / (t * 1e-3) / 1e9 / measured_peaks()["hbm_gbs"], 4),
+            "check_mismatches": check["check_mismatches"]}
+    n, polys = 1 << 17, 1024  # one 131072-point transform of each of 1024 columns (512 MiB), host buffers
+    vals = np.random.default_rng(1).integers(0, P, polys * n, dtype=np.uint32)
+    sq = zoda_b200.PinnedSquare(n, polys)
+    sq.array[:] = vals
+    zoda_b200.ntt_cuda(sq, n, n)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        zoda_b200.ntt_cuda(sq, n, n)
+    ours = (time.perf_counter() - t0) / 3
+    res = {"n": n, "polys": polys, "ours_ms": round(ours * 1e3, 2)}
+    so = os.path.join(ROOT, "oracle", "_ref", "libntt_cuda_ref.so")
+    if os.path.exists(so):
+        ref = ctypes.CDLL(so)
+        ref.cuda_ntt.argtypes = [ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_uint32] * 3
+        import oracle as O
+        roots = O.roots_of_unity(n)
+        sq.array[:] = vals
+        a = sq.array.copy()
+        zoda_b200.ntt_cuda(sq, n, n)
+        ref.cuda_ntt(a.ctypes.data, roots.ctypes.data, n, polys, n)
+        b = sq.array.copy()
+        sq.array[:] = a
+        t0 = time.perf_counter()
+        for _ in range(2):
+            ref.cuda_ntt(sq.array.ctypes.data, roots.ctypes.data, n, polys, n)
+        res["reference_ms"] = round((time.perf_counter() - t0) / 2 * 1e3, 2)
+        res["same_result"] = bool(np.array_equal(a, b))
+    sq.free()
+    out["cuda_ntt_131072"] = res
+    side, cols = 4096, 4096 * SHARE_U32
+    shapes = {}
+    for radix, ctas in ((16, 1), (16, 2), (8, 2), (8, 4)):
+        ctx.plan_set(side, {"impl": 3, "sched": 0, "l2_promo": 3, "blocked": 0, "stagger": 1, "radix": radix,
+                            "ctas": ctas})
+        ms, _, check = time_device_extend(ctx, side, 5, 2, 1, verify=(radix, ctas) == (8, 2), cols=cols)
+        shapes[f"radix{radix}_ctas{ctas}"] = {"ms": round(ms / 5, 4),
+                                              "check_mismatches": check["check_mismatches"] if check else None}
+        torch.cuda.empty_cache()
+    ctx.plan_clear()
+    out["fourstep_side4096"] = shapes
+    return out
 
 
 def time_recover(ctx, k: int, reps: int = 5, seed: int = 3) -> dict:
@@ -333,12 +424,53 @@ def time_encode_general(ctx, k: int, n: int, reps: int = 5) -> dict:
             "gbps": round(k * k * 512 * 8.0 / (ms * 1e-3) / 1e9, 1), "data_rows_ok": ok, "api": api}
 
 
-def time_device_extend(ctx, side: int, steps: int, warmup: int, world: int, sampler=None):
-    """Device-resident extension of one side x side square per step, CUDA events on the launching stream."""
+def data_root_device(rows, slab_bytes: int = 256 << 20) -> str:
+    """compute_data_root (src/benchmarks/utils.rs:51-59) of a row-major u32 device matrix: SHA-256
+    over the little-endian bytes of every row, streamed to the host in slabs of rows."""
+    import hashlib
     import torch
-    cols = side * SHARE_U32
+    nrows, cols = rows.shape
+    per = max(1, slab_bytes // (cols * 4))
+    buf = torch.empty((per, cols), dtype=torch.int32).pin_memory()
+    h = hashlib.sha256()
+    for r0 in range(0, nrows, per):
+        n = min(per, nrows - r0)
+        buf[:n].copy_(rows[r0:r0 + n])
+        h.update(buf[:n].numpy())
+    return h.hexdigest()
+
+
+def verify_extension(ctx, d_in, d_out, side: int, cols: int) -> dict:
+    """The reference's RLC soundness check (src/benchmarks/utils.rs:221-272) over EVERY one of the
+    2*side encoded rows instead of 64 samples: coefficients from the data root of the encoded rows
+    (zoda_rlc_coefficients_device), then zoda_rlc_check_device. 0 mismatches = the output is the
+    extension of the input, each row checked with 4 random-linear-combination limbs."""
+    import torch
+    t0 = time.perf_counter()
+    root = data_root_device(d_out)
+    coeff = torch.empty((cols, 4), dtype=torch.int32, device="cuda")
+    ctx.rlc_coefficients(root, cols, coeff)
+    mm = ctx.rlc_check(d_in, d_out, side, side, cols, coeff)
+    even_ok = bool(torch.equal(d_out[0::2], d_in))
+    del coeff
+    return {"check": f"RLC of all {2 * side} encoded rows (4 limbs each) against the extended RLC of the data, "
+                     "coefficients from the SHA-256 data root of the encoded rows; even rows equal the data",
+            "check_mismatches": int(mm), "even_rows_equal_data": even_ok, "data_root": root,
+            "check_s": round(time.perf_counter() - t0, 2)}
+
+
+def time_device_extend(ctx, side: int, steps: int, warmup: int, world: int, sampler=None, verify: bool = True,
+                       cols: int | None = None):
+    """Device-resident extension of one side x side square per step, CUDA events on the launching stream.
+    With `verify`, the output of the last timed step is checked in full (verify_extension)."""
+    import torch
+    cols = side * SHARE_U32 if cols is None else cols
     gen = torch.Generator(device="cuda").manual_seed(1234 + side)
-    d_in = torch.randint(0, P, (side, cols), dtype=torch.int64, device="cuda", generator=gen).to(torch.int32)
+    d_in = torch.empty((side, cols), dtype=torch.int32, device="cuda")
+    for r0 in range(0, side, 512):  # seeded uniform in [0, p), in slabs to bound the int64 temporary
+        r1 = min(side, r0 + 512)
+        d_in[r0:r1] = torch.randint(0, P, (r1 - r0, cols), dtype=torch.int64, device="cuda",
+                                    generator=gen).to(torch.int32)
     d_out = torch.empty((2 * side, cols), dtype=torch.int32, device="cuda")
     stream = torch.cuda.current_stream()
     for _ in range(warmup):
@@ -359,11 +491,10 @@ def time_device_extend(ctx, side: int, steps: int, warmup: int, world: int, samp
     torch.cuda.synchronize()
     clocks = sampler.stop() if sampler else None
     ms = ev0.elapsed_time(ev1)
-    # spot check of the timed output (even rows are the data)
-    assert torch.equal(d_out[0::2, :256], d_in[:, :256])
+    check = verify_extension(ctx, d_in, d_out, side, cols) if verify else None
     del d_in, d_out
     torch.cuda.empty_cache()
-    return ms, clocks
+    return ms, clocks, check
 
 
 def time_host_extend(ctx, side: int, steps: int, warmup: int):
@@ -385,8 +516,9 @@ def time_host_extend(ctx, side: int, steps: int, warmup: int):
             parts[k] += getattr(t, k)
     # spot check of the last step: even rows are the input, odd rows the extension
     assert torch.equal(h_out[0::2, :64], h_in[:, :64])
-    # PCIe bytes per step: the input up, the odd rows down (even rows are copied on the host)
-    return tot / steps, {k: round(v / steps, 3) for k, v in parts.items()}, side * cols * 4, side * cols * 4
+    # PCIe bytes per step, as the library counted its copies: the input up; the odd rows down, plus
+    # the even rows of the column chunks that return over PCIe (the rest are copied on the host)
+    return tot / steps, {k: round(v / steps, 3) for k, v in parts.items()}, int(t.h2d_bytes), int(t.d2h_bytes)
 
 
 def time_reference_cuda(side: int, iters: int = 2):
@@ -489,10 +621,26 @@ def time_batched(ctx, n: int, hi: int = 2048) -> dict:
             "note": "plain = one zoda_extend_device per square, synchronized (one square at a time)"}
 
 
+def serving_inputs(sides) -> dict:
+    """Pre-staged request payloads in HBM: per side, a pool of distinct squares that together hold at
+    least 256 MiB (twice the L2) and at least two squares, used in rotation, so no request finds its
+    input in L2 from an earlier request of the same side."""
+    import torch
+    pools = {}
+    for s in sorted(set(sides)):
+        nbytes = s * s * SHARE_U32 * 4
+        count = max(2, -(-(256 << 20) // nbytes))
+        pools[s] = [torch.randint(0, P, (s, s * SHARE_U32), dtype=torch.int64, device="cuda").to(torch.int32)
+                    for _ in range(count)]
+    torch.cuda.synchronize()
+    return pools
+
+
 def time_serving(ctx, rate: float, nreq: int, budget_gib: int = 64) -> dict:
     """Seeded Poisson arrivals at `rate` squares/s, sides log-uniform over 64..2048,
-    payloads pre-staged in HBM (one input per side), 64 GiB output budget; p50/p99
-    latency and sustained Gb/s, against the same requests as sequential plain calls."""
+    payloads pre-staged in HBM (serving_inputs: distinct inputs in rotation), 64 GiB output
+    budget; p50/p99 latency and sustained Gb/s, against the same requests as sequential
+    plain calls."""
     import threading
     import numpy as np
     import torch
@@ -500,9 +648,12 @@ def time_serving(ctx, rate: float, nreq: int, budget_gib: int = 64) -> dict:
     rng = np.random.default_rng(1)
     sides = log_uniform_sides(nreq, 64, 2048, seed=1)
     gaps = rng.exponential(1.0 / rate, nreq)
-    inputs = {s: torch.randint(0, P, (s, s * SHARE_U32), dtype=torch.int64, device="cuda").to(torch.int32)
-              for s in sorted(set(sides))}
-    torch.cuda.synchronize()
+    pools = serving_inputs(sides)
+    seen = {s: 0 for s in pools}
+    req_in = []
+    for s in sides:  # request i's input: the next square of its side's pool
+        req_in.append(pools[s][seen[s] % len(pools[s])])
+        seen[s] += 1
     srv = zoda_b200.Server(ctx, budget_bytes=budget_gib << 30, max_inflight=4, max_batch=128)
     tickets = [None] * nreq
     submitted = threading.Event()
@@ -516,7 +667,7 @@ def time_serving(ctx, rate: float, nreq: int, budget_gib: int = 64) -> dict:
                 if dt <= 0:
                     break
                 time.sleep(dt if dt < 2e-4 else dt - 1e-4)
-            tickets[i] = srv.submit(inputs[s], s, s * SHARE_U32)
+            tickets[i] = srv.submit(req_in[i], s, s * SHARE_U32)
         submitted.set()
 
     old_switch = sys.getswitchinterval()
@@ -538,14 +689,14 @@ def time_serving(ctx, rate: float, nreq: int, budget_gib: int = 64) -> dict:
     srv.close()
     payload = sum(payload_bits(s) for s in sides)
     # the same requests as plain sequential calls
-    outs = {s: torch.empty((2 * s, s * SHARE_U32), dtype=torch.int32, device="cuda") for s in inputs}
+    outs = {s: torch.empty((2 * s, s * SHARE_U32), dtype=torch.int32, device="cuda") for s in pools}
     torch.cuda.synchronize()
     t1 = time.perf_counter()
-    for s in sides:
-        ctx.extend(inputs[s], outs[s], s, s * SHARE_U32)
+    for i, s in enumerate(sides):
+        ctx.extend(req_in[i], outs[s], s, s * SHARE_U32)
         torch.cuda.synchronize()
     tplain = time.perf_counter() - t1
-    del inputs, outs
+    del pools, req_in, outs
     torch.cuda.empty_cache()
     lat.sort()
     return {"requests": nreq, "offered_rate_per_s": rate, "offered_gbps": round(payload / (gaps.sum()) / 1e9, 1),
@@ -553,7 +704,70 @@ def time_serving(ctx, rate: float, nreq: int, budget_gib: int = 64) -> dict:
             "p50_ms": round(st.p50_ms, 3), "p99_ms": round(st.p99_ms, 3), "max_ms": round(st.max_ms, 3),
             "launches": int(st.launches), "wall_s": round(wall, 3),
             "plain_sequential_gbps": round(payload / tplain / 1e9, 1),
-            "budget_gib": budget_gib, "sides": "log-uniform 64..2048, 128 u32/share, seed 1"}
+            "budget_gib": budget_gib, "sides": "log-uniform 64..2048, 128 u32/share, seed 1",
+            "inputs": "distinct pre-staged squares per side, >= 256 MiB per side, in rotation"}
+
+
+def workload_config(side: int) -> dict:
+    """The workload both arms name (identical dicts, so the two lines compare like for like)."""
+    cols = side * SHARE_U32
+    return {"workload": f"plain extension of one {side}x{side} square of 512-byte shares per GPU "
+                        f"([{side}][{cols}] u32 -> [{2 * side}][{cols}])",
+            "side": side, "cols": cols, "share_bytes": 512,
+            "l2": "inputs and outputs larger than the 126 MB L2; no flush between steps"}
+
+
+def launches_per_step(side: int, plan: dict | None) -> int:
+    """Kernels zoda_extend_device launches per square: the four-step plan (and every side above
+    4096) runs three passes, the single-pass kernels one."""
+    if side > 4096 or (plan and plan.get("impl") == 3):
+        return 3
+    return 1
+
+
+def plan_kernels(side: int, plan: dict | None) -> str:
+    if side > 4096 or (plan and plan.get("impl") == 3):
+        return "k_step / k_step2 (three four-step passes: strided INTT, block INTT+twist+NTT, strided NTT)"
+    return kernel_name(side, plan)
+
+
+def measure_side(ctx, side: int, steps: int, warmup: int, world: int, sampler=None, tune_it: bool = True,
+                 e2e_steps: int = 3, cpu_budget: float = 0.0) -> dict:
+    """Everything the JSON line says about one square size: the side's plan (tuned at this workload),
+    device-resident payload Gb/s over `steps` timed steps (max over ranks), the HBM roofline of the
+    step, the full check of the timed output, the same extension end to end through the host-buffer
+    C ABI call, and (cpu_budget > 0) the CPU port on a bounded column sample."""
+    cols = side * SHARE_U32
+    plan = tune(ctx, side, cols, reps=3 if side >= 4096 else 10) if tune_it else None
+    ms, clocks, check = time_device_extend(ctx, side, steps, warmup, world, sampler)
+    ms_max = max_over_ranks(ms, world)
+    peaks = measured_peaks()
+    alg_bytes = 12.0 * side * cols  # read [side][cols] + write [2 side][cols] u32, the single-pass minimum
+    achieved = alg_bytes / (ms / steps * 1e-3) / 1e9
+    barrier(world)
+    e2e_ms, parts, h2d, d2h = time_host_extend(ctx, side, e2e_steps, 1)
+    e2e_max = max_over_ranks(e2e_ms, world)
+    out = {
+        "value": job_rate(world, side, ms_max, steps), "ms_per_step": ms_max / steps, "plan": plan,
+        "plan_source": "zoda_autotune at this workload" if plan else "default",
+        "clocks": clocks, "output_check": check,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": round(achieved / peaks["hbm_gbs"], 4),
+                     "traffic": ncu_traffic(f"k_extend_side{side}" + ("_fourstep" if launches_per_step(side, plan) == 3
+                                                                       else "")),
+                     "peak_source": peaks["source"], "kernel": plan_kernels(side, plan),
+                     "launches_per_step": launches_per_step(side, plan), "alg_bytes_per_step": alg_bytes},
+        "e2e": {"value": round(job_rate(world, side, e2e_max, 1), 3), "unit": "Gb/s",
+                "h2d_bytes_per_step": world * h2d, "d2h_bytes_per_step": world * d2h,
+                "ms_per_step": round(e2e_max, 3), "split_ms": parts,
+                "api": "zoda_extend_host (pinned host buffers; odd rows over PCIe, even rows copied on the host "
+                       "except the last eighth of the column chunks)"},
+    }
+    if cpu_budget > 0:
+        cpu = cpu_port_rate(side, cpu_budget)
+        cpu.pop("seconds", None)
+        out["cpu_baseline"] = cpu
+    return out
 
 
 def run_ours(args, world, rank, local):
@@ -567,42 +781,26 @@ def run_ours(args, world, rank, local):
                                 device_id=torch.device("cuda", local))
     ctx = zoda_b200.Context(local)
     side = args.side
-    cols = side * SHARE_U32
-    plan = None if args.no_tune else tune(ctx, side, cols, reps=10)
     sampler = ClockSampler(local) if rank == 0 else None
-    ms, clocks = time_device_extend(ctx, side, args.steps, args.warmup, world, sampler)
-    ms_max = max_over_ranks(ms, world)
-    t_step = ms_max / args.steps
-    value = job_rate(world, side, ms_max, args.steps)
-    alg_bytes = 12.0 * side * cols  # read [side][cols] + write [2 side][cols] u32
-    peaks = measured_peaks()
-    achieved = alg_bytes / (ms / args.steps * 1e-3) / 1e9
-    traffic = ncu_traffic(f"k_extend_side{side}")
+    # the headline: every rank extends its own square; the CPU baseline runs on rank 0 of a 1-GPU run only
+    head = measure_side(ctx, side, args.steps, args.warmup, world, sampler, tune_it=not args.no_tune,
+                        e2e_steps=max(2, min(args.steps, 3)),
+                        cpu_budget=args.cpu_budget if rank == 0 and world == 1 else 0.0)
     extra = {}
-    cpu = None
-    # e2e: every rank encodes its own square from host buffers at the same time; the slowest sets the step
-    barrier(world)
-    e2e_ms, parts, h2d, d2h = time_host_extend(ctx, side, max(2, min(args.steps, 5)), 1)
-    e2e_max = max_over_ranks(e2e_ms, world)
-    e2e = {"value": round(job_rate(world, side, e2e_max, 1), 3), "unit": "Gb/s",
-           "h2d_bytes_per_step": world * h2d, "d2h_bytes_per_step": world * d2h, "ms_per_step": round(e2e_max, 3),
-           "split_ms": parts,
-           "api": "zoda_extend_host (pinned host buffers; odd rows over PCIe, even rows copied on the host)"}
     if world > 1:
         barrier(world)
-    # report-only extras and the CPU baseline: rank 0 of a 1-GPU run only (they would hold the other
-    # ranks at the next barrier for a minute or more)
+    # report-only extras: rank 0 of a 1-GPU run only (they would hold the other ranks at the next
+    # barrier for a minute or more)
     if rank == 0 and world == 1 and not args.no_extra:
         for s2 in args.extra_sides:
             if s2 == side:
                 continue
-            plan2 = None if args.no_tune else tune(ctx, s2, s2 * SHARE_U32, reps=3 if s2 >= 4096 else 6)
-            ms2, _ = time_device_extend(ctx, s2, max(3, args.steps // 2), 3, 1)
-            t2 = ms2 / max(3, args.steps // 2)
-            extra[f"side{s2}"] = {
-                "ms_per_step": round(t2, 4), "gbps": round(payload_bits(s2) / (t2 * 1e-3) / 1e9, 1),
-                "hbm_frac": round(12.0 * s2 * s2 * SHARE_U32 / (t2 * 1e-3) / 1e9 / peaks["hbm_gbs"], 4),
-                "kernel": kernel_name(s2, plan2), "plan": plan2}
+            m = measure_side(ctx, s2, args.steps, args.warmup, 1, tune_it=not args.no_tune, e2e_steps=3,
+                             cpu_budget=args.cpu_budget / 2 if s2 == 1024 else 0.0)
+            m["gbps"] = round(m.pop("value"), 1)
+            m["ms_per_step"] = round(m["ms_per_step"], 4)
+            m["config"] = workload_config(s2)
+            extra[f"side{s2}"] = m
         extra["recover_k1024"] = time_recover(ctx, 1024)
         extra["encode_k1000_n1000"] = time_encode_general(ctx, 1000, 1000)
         extra["encode_k1000_n3000"] = time_encode_general(ctx, 1000, 3000)
@@ -617,33 +815,29 @@ def run_ours(args, world, rank, local):
             # where launch overhead dominates: the same draw restricted to sides 32..256
             extra["batched_small_squares"] = time_batched(ctx, args.batch_squares, hi=256)
             extra["serving"] = time_serving(ctx, args.serve_rate, args.serve_requests)
-    if rank == 0 and world == 1:
-        cpu = cpu_port_rate(side, args.cpu_budget)
-        cpu.pop("seconds", None)
-        if not args.no_extra:  # the port on one thread, as the reference's CPU path runs
-            one = cpu_port_rate(side, max(2.0, args.cpu_budget / 4), threads=1)
-            one.pop("seconds", None)
-            extra["cpu_port_single_thread"] = one
+            # below capacity: latency without queueing behind a saturated device
+            extra["serving_below_capacity"] = time_serving(ctx, args.serve_rate / 2, args.serve_requests)
+        one = cpu_port_rate(side, max(2.0, args.cpu_budget / 4), threads=1)  # as the reference's CPU path runs
+        one.pop("seconds", None)
+        extra["cpu_port_single_thread"] = one
     if world > 1:
         barrier(world)
     if rank == 0:
+        check = head["output_check"]
         line = {
-            "metric": METRIC, "value": round(value, 3), "unit": "Gb/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(t_step, 4), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded uniform in [0,p), device-resident)",
-            "config": {"workload": f"plain device-resident extension of one {side}x{side} square per GPU "
-                                   f"([{side}][{cols}] u32 -> [{2 * side}][{cols}])",
-                       "side": side, "cols": cols, "share_bytes": 512,
-                       "plan": plan, "plan_source": "zoda_autotune at this workload" if plan else "default",
-                       "l2": "inputs (and outputs) larger than the 126 MB L2; no flush"},
-            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
-                         "peak_source": peaks["source"], "kernel": kernel_name(side, plan),
-                         "alg_bytes_per_launch": alg_bytes},
-            "cpu_baseline": cpu,
-            "e2e": e2e,
-            "gpu_launches": args.steps,
-            "clocks": clocks,
+            "metric": METRIC, "value": round(head["value"], 3), "unit": "Gb/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(head["ms_per_step"], 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded uniform in [0,p), device-resident)",
+            "config": workload_config(side),
+            "plan": head["plan"], "plan_source": head["plan_source"],
+            "roofline": head["roofline"],
+            "cpu_baseline": head.get("cpu_baseline"),
+            "check_mismatches": check["check_mismatches"] if check else None,
+            "output_check": check,
+            "e2e": head["e2e"],
+            "gpu_launches": args.steps * head["roofline"]["launches_per_step"],
+            "clocks": head["clocks"],
             "extra": extra,
         }
         print(json.dumps(line), flush=True)
@@ -659,8 +853,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--side", type=int, default=1024)
-    ap.add_argument("--extra-sides", type=int, nargs="*", default=[2048, 4096])
+    ap.add_argument("--side", type=int, default=4096,
+                    help="the headline square (default: 4096, the largest single-GPU configuration)")
+    ap.add_argument("--extra-sides", type=int, nargs="*", default=[1024, 2048])
     ap.add_argument("--no-extra", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched and serving report lines")
     ap.add_argument("--no-tune", action="store_true", help="run the default plans instead of tuning first")
@@ -670,15 +865,24 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=10.0, help="seconds of CPU baseline sampling")
     ap.add_argument("--ref-step-budget", type=float, default=None,
                     help="seconds of CPU work per step of --impl reference (default: about 60 s in total)")
-    ap.add_argument("--leg", choices=["rlc", "recover", "encode"], default=None,
-                    help="run one report-only leg on one GPU and print its JSON (a small case to profile)")
+    ap.add_argument("--leg", choices=["rlc", "recover", "encode", "extend", "footprint", "long"], default=None,
+                    help="run one report-only leg on one GPU and print its JSON (a small case to profile): "
+                         "extend = --steps extensions of a [--side][--cols] slab; footprint = ps per element "
+                         "of the --side extension against the number of columns")
+    ap.add_argument("--cols", type=int, default=0, help="columns of the extend leg (0: side * 128)")
+    ap.add_argument("--force-impl", choices=["auto", "direct", "tma"], default="auto",
+                    help="legs only: run one kernel family with default knobs instead of the side's plan")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps
     if args.leg:
         import zoda_b200
         ctx = zoda_b200.Context(0)
+        ctx.set_impl({"auto": 0, "direct": 1, "tma": 2}[args.force_impl])
         leg = {"rlc": lambda: time_rlc(ctx, 1024), "recover": lambda: time_recover(ctx, 1024),
-               "encode": lambda: [time_encode_general(ctx, 1000, 1000), time_encode_general(ctx, 1000, 3000)]}[args.leg]
+               "encode": lambda: [time_encode_general(ctx, 1000, 1000), time_encode_general(ctx, 1000, 3000)],
+               "extend": lambda: time_extend_leg(ctx, args.side, args.cols or args.side * SHARE_U32, args.steps,
+                                                 args.warmup),
+               "footprint": lambda: footprint_sweep(ctx, args.side), "long": lambda: time_long_leg(ctx)}[args.leg]
         res = leg()
         print(json.dumps({"leg": args.leg, **res} if isinstance(res, dict) else {"leg": args.leg, "runs": res}))
         return

@@ -84,16 +84,18 @@ const char* zoda_last_error(void);
 zoda_status zoda_ctx_create(int device, zoda_ctx** out);
 void zoda_ctx_destroy(zoda_ctx* ctx);
 
-/* Largest k the fused extension accepts (4096). */
+/* Largest k the extension accepts (2^26): one fused pass up to 4096, three
+ * four-step passes above (no column of more than 4096 rows fits on chip). */
 uint32_t zoda_max_side(void);
 
 /* Kernel variant of the fused extension on a context. AUTO runs the side's
  * plan (below); the others force one kernel with default knobs (for tests;
- * TMA supports k in [32, 4096]). */
+ * TMA supports k in [32, 4096], FOURSTEP k in [1024, 4096]). */
 typedef enum zoda_extend_impl {
     ZODA_IMPL_AUTO = 0,
     ZODA_IMPL_DIRECT = 1,
-    ZODA_IMPL_TMA = 2
+    ZODA_IMPL_TMA = 2,
+    ZODA_IMPL_FOURSTEP = 3 /* three passes of sqrt(k)-point transforms, as above 4096 */
 } zoda_extend_impl;
 zoda_status zoda_ctx_set_impl(zoda_ctx* ctx, int impl);
 
@@ -105,7 +107,8 @@ zoda_status zoda_ctx_set_impl(zoda_ctx* ctx, int impl);
  * stagger 1, radix 16). Every plan computes the same bits; only the speed
  * differs. */
 typedef struct zoda_plan {
-    int32_t impl;     /* ZODA_IMPL_DIRECT or ZODA_IMPL_TMA (k >= 32)                   */
+    int32_t impl;     /* ZODA_IMPL_DIRECT, ZODA_IMPL_TMA (k >= 32) or ZODA_IMPL_FOURSTEP
+                         (1024 <= k <= 4096)                                          */
     int32_t sched;    /* direct kernel: the leftover radix at the INTT's last level (0)
                          or its first level (1)                                        */
     int32_t l2_promo; /* TMA kernel: L2 promotion of tile loads, 0 none, 1 64 B,
@@ -118,6 +121,9 @@ typedef struct zoda_plan {
                          (1024 threads, 8 positions: twice the warps; direct kernel
                          from k = 64)                                              */
     float ms;         /* the tuner's time for this plan (0 when set by hand)            */
+    int32_t ctas;     /* FOURSTEP: CTAs resident per SM in its passes, 1 (512 threads),
+                         2 (256 threads at radix 16, 512 at radix 8) or 4 (256 threads,
+                         radix 8); 0 counts as 1. Ignored by the other kernels.    */
 } zoda_plan;
 
 /* Times every candidate plan for each power-of-two side in [side_min,
@@ -164,10 +170,13 @@ zoda_status zoda_extend_device(zoda_ctx* ctx, const uint32_t* d_in, uint32_t* d_
  * different column chunks overlap, so the three busy times (CUDA events) can
  * add up to more than total_ms. */
 typedef struct zoda_timing {
-    float h2d_ms;    /* host -> device copies of the input, summed          */
-    float kernel_ms; /* fused extension kernels, summed                     */
-    float d2h_ms;    /* device -> host copies of the odd output rows, summed */
-    float total_ms;  /* the whole call, host wall clock                     */
+    float h2d_ms;       /* host -> device copies of the input, summed              */
+    float kernel_ms;    /* fused extension kernels, summed                         */
+    float d2h_ms;       /* device -> host copies of output rows, summed            */
+    float total_ms;     /* the whole call, host wall clock                         */
+    uint64_t h2d_bytes; /* bytes the call copied host -> device                    */
+    uint64_t d2h_bytes; /* bytes the call copied device -> host (odd rows, plus the
+                           even rows of the chunks that return over PCIe)           */
 } zoda_timing;
 
 /* Fused extension from host memory to host memory: the reference's
@@ -176,11 +185,23 @@ typedef struct zoda_timing {
  * [k][cols], h_out row-major [2k][cols]; pinned buffers give full PCIe speed.
  * The square moves in column chunks over three streams, so uploads,
  * kernels and downloads overlap; device buffers are the context's cached
- * chunk buffers. Only the odd output rows cross PCIe: the even rows equal the
- * input rows and host threads copy them meanwhile. Synchronous. `timing` may
- * be NULL. */
+ * chunk buffers. The odd output rows cross PCIe; the even rows equal the
+ * input rows, and host threads copy most of them meanwhile (those of the last
+ * eighth of the column chunks come back over PCIe instead). Synchronous,
+ * also on failure: an error return happens only after every copy the call
+ * queued has finished, so the caller may free its buffers at once. `timing`
+ * may be NULL. */
 zoda_status zoda_extend_host(zoda_ctx* ctx, const uint32_t* h_in, uint32_t* h_out, uint32_t k, uint64_t cols,
                              zoda_timing* timing);
+
+/* Fault injection for tests of the error paths; no counterpart in the
+ * reference. Arms `site`: the call passes through it `after` more times, then
+ * the next pass fails with ZODA_ERR_CUDA (zoda_last_error says "injected
+ * fault") and the site disarms. site 0 disarms everything. Sites:
+ *   ZODA_FAULT_HOST_CHUNK  the launch of one column chunk in zoda_extend_host,
+ *                          after earlier chunks' copies have been queued. */
+#define ZODA_FAULT_HOST_CHUNK 1u
+zoda_status zoda_ctx_inject_fault(zoda_ctx* ctx, uint32_t site, uint32_t after);
 
 /* ----------------------------------------------------------------------
  * Batched extension: many squares of mixed sides in one persistent launch.
@@ -364,12 +385,13 @@ zoda_status zoda_rlc_check_device(zoda_ctx* ctx, const uint32_t* d_data, const u
  * and stall other streams. The call performs no cudaMalloc, no cudaFree and
  * no allocating library call; the caller passes the input and the output.
  *
- * What it computes: the cuda_ntt (inverse = 0) or cuda_intt (inverse = 1)
- * transform, with the standard roots [w^0 .. w^(n-1)], w = 31^((p-1)/n), of
- * `polys` polynomials of n canonical u32 each, laid end to end in device
- * memory (polynomial c at d_in[c*n .. c*n + n)), written the same way to
- * d_out (d_out may equal d_in). n must be a power of two <= 4096.
- * Asynchronous on `stream` (NULL = the legacy default stream).
+ * What it computes: for each of `polys` polynomials of n canonical u32,
+ * laid end to end in device memory (polynomial c at d_in[c*n .. c*n + n)),
+ *   d_out[c*n + k] = scale * sum_{i<n} d_in[c*n + i] * w^(s*i*k)  mod p,
+ * with w = 31^((p-1)/n), s = +1 and scale = 1 when inverse = 0, and
+ * s = -1 and scale = n^-1 mod p when inverse = 1 (natural order in and
+ * out, canonical results). d_out may equal d_in. n must be a power of two
+ * <= 4096. Asynchronous on `stream` (NULL = the legacy default stream).
  *
  * Limits: the working copy lives in a fixed 16 MiB device array inside the
  * library, so n * round_up(polys, 4) must be <= 4194304 u32; larger requests

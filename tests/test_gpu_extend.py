@@ -169,7 +169,7 @@ def test_extend_rejects_bad_arguments(ctx):
         ctx.extend(a, b, 4, 62)  # cols not a multiple of 4
     assert e.value.status == 1
     with pytest.raises(zoda_b200.ZodaError) as e:
-        ctx.extend(a, b, 8192, 4)  # beyond the largest side
+        ctx.extend(a, b, 1 << 27, 4)  # beyond the largest side (2^26)
     assert e.value.status == 4
     with pytest.raises(zoda_b200.ZodaError):
         ctx.extend(a, a, 2, 64)  # output overlaps input

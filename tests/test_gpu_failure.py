@@ -32,3 +32,34 @@ def test_bounded_wait_is_reported_and_the_context_survives():
         c.check()
     finally:
         c.close()
+
+
+def test_host_call_error_returns_with_no_copy_outstanding():
+    """A column chunk of zoda_extend_host fails mid-call (injected after two chunks
+    have queued their copies): the call reports the failure only once every copy it
+    queued has finished, so nothing lands in the caller's output after it returns;
+    the next call on the same context is bit-exact."""
+    import time
+
+    import zoda_b200
+    side, cols = 64, 1 << 20  # 256 MiB of input: four 64 MiB column chunks
+    c = zoda_b200.Context(0)
+    try:
+        data = O.seeded_input(side, 4096, seed=8)
+        h_in = torch.from_numpy(np.tile(data, (1, cols // 4096)).view(np.int32)).pin_memory()
+        h_out = torch.zeros((2 * side, cols), dtype=torch.int32).pin_memory()
+        c.inject_fault(1, after=2)
+        with pytest.raises(zoda_b200.ZodaError) as e:
+            c.extend_host(h_in, h_out, side, cols)
+        assert e.value.status == 2 and "injected" in str(e.value)
+        h_out.fill_(-7)  # after the return nothing may write here any more
+        time.sleep(0.3)
+        assert bool((h_out == -7).all())
+        t = c.extend_host(h_in, h_out, side, cols)  # the fault disarmed itself
+        want = O.encode_rowmajor(data)
+        got = h_out.numpy().view(np.uint32)
+        for c0 in (0, cols // 2, cols - 4096):
+            assert np.array_equal(got[:, c0:c0 + 4096], want)
+        assert t.h2d_bytes == side * cols * 4 and t.d2h_bytes >= side * cols * 4
+    finally:
+        c.close()

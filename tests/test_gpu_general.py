@@ -124,7 +124,7 @@ def test_encode_bad_args(ctx):
         ctx.encode(d, o, 8, 8, 6)       # cols not a multiple of 4
     big = torch.zeros((4, 8), dtype=torch.int32, device="cuda")
     with pytest.raises(zoda_b200.ZodaError):
-        ctx.encode(big, o, 5000, 1, 8)  # next_pow2(k) > 4096
+        ctx.encode(big, o, (1 << 26) + 1, 1, 8)  # next_pow2(k) > 2^26
 
 
 # ---- decoder -------------------------------------------------------------------
@@ -223,4 +223,4 @@ def test_recover_bad_args(ctx):
         ctx.recover(code, range(k), 12, cols, out)              # k not a power of two
     big = torch.zeros((8, 8), dtype=torch.int32, device="cuda")
     with pytest.raises(zoda_b200.ZodaError):
-        ctx.recover(big, range(8192), 8192, 8, big)             # beyond k = 4096
+        ctx.recover(big, range(8), 1 << 27, 8, big)             # beyond the largest k

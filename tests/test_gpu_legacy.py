@@ -98,6 +98,18 @@ def test_legacy_seeded_many_polys(zb, log_n, inverse):
     assert np.array_equal(got, O.ntt_polys(vals, n, stride, inverse))
 
 
+@pytest.mark.parametrize("log_n,polys", [(1, (1 << 21) + 5), (2, (1 << 22) + 3)])
+def test_legacy_many_short_polys(zb, log_n, polys):
+    # more than 65535 32-polynomial tiles in one device chunk (the transposes walk them with a grid stride)
+    n = 1 << log_n
+    rng = np.random.default_rng(polys)
+    vals = rng.integers(0, P, polys * n, dtype=np.uint32)
+    for inverse in (False, True):
+        got = vals.copy()
+        (zb.intt_cuda if inverse else zb.ntt_cuda)(got, n, n)
+        assert np.array_equal(got, O.ntt_polys(vals, n, n, inverse))
+
+
 def test_legacy_zoda_extend_two_calls(zb):
     # src/zoda/babybear.rs:34-39 GPU branch: intt over n_k inside n_kn-tall columns, then ntt over n_kn
     k, cols = 32, 40

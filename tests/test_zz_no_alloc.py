@@ -5,13 +5,18 @@ fixed array inside the library instead of allocating.
 
 Checked through the C ABI against the existing entry points cuda_ntt /
 cuda_intt on the same inputs, bit-exact, over two calls in a row (the array
-keeps the previous call's contents, so the second call must not see them).
+keeps the previous call's contents, so the second call must not see them),
+and directly against the CPU oracle's restatement of the reference's
+transform (src/ntt/cpu.rs:1-60), including the largest accepted request at
+n = 2 (2^21 polynomials, more 32-row tiles than a grid's y dimension holds).
 This file is collected last so that a run stopping at its first failure has
 run every other test first; it also passes alone in a fresh process."""
 import ctypes
 
 import numpy as np
 import pytest
+
+import oracle as O
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
@@ -55,11 +60,25 @@ def test_noalloc_matches_existing_entry_two_calls(zb, n, polys, inverse):
         assert np.array_equal(got, want), f"call {call}"
 
 
+@pytest.mark.parametrize("n,polys", [(2, 2097152), (2, 2097149), (4, 1048573), (8, 1000), (4096, 1021)])
+@pytest.mark.parametrize("inverse", [False, True])
+def test_noalloc_matches_oracle(zb, n, polys, inverse):
+    # the CPU oracle (src/ntt/cpu.rs restated), up to the array's limit: n * round_up(polys, 4) = 4 Mi u32
+    assert n * ((polys + 3) // 4 * 4) <= MAX_ELEMS
+    rng = np.random.default_rng(n + polys + 11 * int(inverse))
+    for call in range(2):
+        vals = rng.integers(0, P, n * polys, dtype=np.uint32)
+        got = noalloc(zb, vals, n, polys, inverse)
+        assert np.array_equal(got, O.ntt_polys(vals, n, n, inverse)), f"call {call}"
+
+
 def test_noalloc_rejects_requests_beyond_its_array(zb):
     lib = zb.load()
     d = torch.empty(8, dtype=torch.int32, device="cuda")
     # 4096 * 1028 u32 is more than the 4194304-element array
     assert lib.zoda_ntt_device_noalloc(d.data_ptr(), d.data_ptr(), 4096, 1025, 0, None) == 4
     assert b"exceeds" in lib.zoda_last_error()
+    # one polynomial past the limit at n = 2
+    assert lib.zoda_ntt_device_noalloc(d.data_ptr(), d.data_ptr(), 2, 2097153, 0, None) == 4
     assert lib.zoda_ntt_device_noalloc(d.data_ptr(), d.data_ptr(), 8192, 1, 0, None) == 4
     assert lib.zoda_ntt_device_noalloc(d.data_ptr(), d.data_ptr(), 48, 1, 0, None) == 1

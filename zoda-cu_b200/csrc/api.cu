@@ -193,7 +193,7 @@ const char* zoda_status_string(zoda_status s) {
 
 const char* zoda_last_error(void) { return g_last_error.c_str(); }
 
-uint32_t zoda_max_side(void) { return 4096u; }
+uint32_t zoda_max_side(void) { return 1u << LONG_MAX_LOG; }
 
 zoda_status zoda_ctx_create(int device, zoda_ctx** out) {
     if (!out) return ZODA_ERR_ARG;
@@ -237,6 +237,22 @@ zoda_status zoda_ctx_create(int device, zoda_ctx** out) {
         set_last_error("cudaMemcpy(tables)", e);
         return fail(ZODA_ERR_CUDA);
     }
+    {
+        // omega_{2^26}^j for j < 8192: the low half of the two-level root table of the long-column passes
+        std::vector<Tw> lo(8192);
+        const uint32_t w = root_of_unity(26);
+        uint32_t cur = 1;
+        for (auto& x : lo) {
+            x = Tw{cur, shoup(cur)};
+            cur = mulmod_c(cur, w);
+        }
+        if ((e = cudaMalloc(&c->tables.tw_lo, lo.size() * sizeof(Tw))) != cudaSuccess ||
+            (e = cudaMemcpy(c->tables.tw_lo, lo.data(), lo.size() * sizeof(Tw), cudaMemcpyHostToDevice)) !=
+                cudaSuccess) {
+            set_last_error("cudaMalloc(tw_lo)", e);
+            return fail(ZODA_ERR_NOMEM);
+        }
+    }
     if ((e = cudaMalloc(&c->d_err, sizeof(int))) != cudaSuccess || (e = cudaMemset(c->d_err, 0, sizeof(int))) != cudaSuccess) {
         set_last_error("cudaMalloc(err)", e);
         return fail(ZODA_ERR_NOMEM);
@@ -254,6 +270,7 @@ zoda_status zoda_ctx_create(int device, zoda_ctx** out) {
     }
     zoda_status s = extend_init_attributes();
     if (s == ZODA_OK) s = rlc_init_attributes();
+    for (int L = FOURSTEP_MIN_LOG; L <= 12 && s == ZODA_OK; L++) s = coset_mid_tables(c, L, L + 1, &c->tables.ext4[L]);
     if (s != ZODA_OK) return fail(s);
     *out = c;
     return ZODA_OK;
@@ -276,6 +293,7 @@ void zoda_ctx_destroy(zoda_ctx* c) {
     rlc_release(c);
     if (c->d_err) cudaFree(c->d_err);
     if (c->tables.tw) cudaFree(c->tables.tw);
+    if (c->tables.tw_lo) cudaFree(c->tables.tw_lo);
     if (c->tables.twist) cudaFree(c->tables.twist);
     if (c->tables.side) cudaFree(c->tables.side);
     for (auto& ev : c->ev)
@@ -307,11 +325,27 @@ zoda_status zoda_extend_device(zoda_ctx* ctx, const uint32_t* d_in, uint32_t* d_
     if (a < b + 2 * in_bytes && b < a + in_bytes) return ZODA_ERR_ARG;  // overlap
     if (cols == 0) return ZODA_OK;
     ZB_CUDA(cudaSetDevice(ctx->device));
+    if (ls > 12) {  // no column fits one pass: three four-step passes
+        const uint2* tabs = nullptr;
+        {
+            std::lock_guard<std::mutex> lock(ctx->mu);  // the context's table map
+            if ((s = coset_mid_tables(ctx, ls, ls + 1, &tabs)) != ZODA_OK) return s;
+        }
+        return long_extend(ctx, ls, tabs, d_in, d_out, cols, (cudaStream_t)stream);
+    }
     return launch_extend(ctx, ls, d_in, d_out, cols, (cudaStream_t)stream, ctx->impl);
 }
 
+zoda_status zoda_ctx_inject_fault(zoda_ctx* ctx, uint32_t site, uint32_t after) {
+    if (!ctx || site > ZODA_FAULT_HOST_CHUNK) return ZODA_ERR_ARG;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->fault_site = site;
+    ctx->fault_after = after;
+    return ZODA_OK;
+}
+
 zoda_status zoda_ctx_set_impl(zoda_ctx* ctx, int impl) {
-    if (!ctx || impl < 0 || impl > 2) return ZODA_ERR_ARG;
+    if (!ctx || impl < 0 || impl > 3) return ZODA_ERR_ARG;
     ctx->impl = impl;
     return ZODA_OK;
 }
@@ -371,43 +405,70 @@ zoda_status zoda_extend_host(zoda_ctx* ctx, const uint32_t* h_in, uint32_t* h_ou
     if (dev_even >= nch) dev_even = nch - 1;
     const uint64_t host_cols = (nch - dev_even) * cw < cols ? (nch - dev_even) * cw : cols;
     EvenRowCopy even(h_in, h_out, k, cols, host_cols);
-    for (int i = 0; i < zoda_ctx::NHS; i++) {
-        if (!ctx->hs[i]) ZB_CUDA(cudaStreamCreateWithFlags(&ctx->hs[i], cudaStreamNonBlocking));
-        if ((s = ctx->hin[i].ensure((size_t)k * cw * 4)) != ZODA_OK) return s;
-        if ((s = ctx->hout[i].ensure((size_t)k * cw * 4)) != ZODA_OK) return s;
-    }
-    for (uint64_t c = 0; c < nch; c++)
-        for (auto& e : ctx->cev[c])
-            if (!e) ZB_CUDA(cudaEventCreate(&e));
-    // all streams start after ev[0]
-    ZB_CUDA(cudaEventRecord(ctx->ev[0], ctx->hs[0]));
-    for (int i = 1; i < zoda_ctx::NHS; i++) ZB_CUDA(cudaStreamWaitEvent(ctx->hs[i], ctx->ev[0], 0));
-    for (uint64_t c = 0; c < nch; c++) {
-        const int b = (int)(c % zoda_ctx::NHS);
-        cudaStream_t st = ctx->hs[b];
-        const uint64_t c0 = c * cw, w = (cols - c0 < cw) ? cols - c0 : cw;
-        uint32_t* din = (uint32_t*)ctx->hin[b].p;
-        uint32_t* dout = (uint32_t*)ctx->hout[b].p;
-        cudaEvent_t* e = ctx->cev[c];
-        ZB_CUDA(cudaEventRecord(e[0], st));
-        ZB_CUDA(cudaMemcpy2DAsync(din, w * 4, h_in + c0, cols * 4, w * 4, k, cudaMemcpyHostToDevice, st));
-        ZB_CUDA(cudaEventRecord(e[1], st));
-        if ((s = launch_extend(ctx, ls, din, dout, w, st, ctx->impl, true)) != ZODA_OK) return s;
-        ZB_CUDA(cudaEventRecord(e[2], st));
-        // odd rows 1, 3, .. of the output: a stride of two output rows
-        ZB_CUDA(cudaMemcpy2DAsync(h_out + cols + c0, 2 * cols * 4, dout, w * 4, w * 4, (size_t)k,
-                                  cudaMemcpyDeviceToHost, st));
-        if (c0 >= host_cols)  // even rows 0, 2, .. of this chunk: the uploaded input, before the buffer is reused
-            ZB_CUDA(cudaMemcpy2DAsync(h_out + c0, 2 * cols * 4, din, w * 4, w * 4, (size_t)k,
+    uint64_t h2d_bytes = 0, d2h_bytes = 0;
+    // Everything that queues copies into the caller's buffers. On a failure the
+    // streams are drained before the status is returned, so no copy queued
+    // here lands in h_out (or reads h_in) after the call has returned.
+    auto pipeline = [&]() -> zoda_status {
+        zoda_status r;
+        for (int i = 0; i < zoda_ctx::NHS; i++) {
+            if (!ctx->hs[i]) ZB_CUDA(cudaStreamCreateWithFlags(&ctx->hs[i], cudaStreamNonBlocking));
+            if ((r = ctx->hin[i].ensure((size_t)k * cw * 4)) != ZODA_OK) return r;
+            if ((r = ctx->hout[i].ensure((size_t)k * cw * 4)) != ZODA_OK) return r;
+        }
+        for (uint64_t c = 0; c < nch; c++)
+            for (auto& e : ctx->cev[c])
+                if (!e) ZB_CUDA(cudaEventCreate(&e));
+        const uint2* long_tabs = nullptr;  // sides above 4096: the three-pass extension's factor tables
+        if (ls > 12 && (r = coset_mid_tables(ctx, ls, ls + 1, &long_tabs)) != ZODA_OK) return r;
+        // all streams start after ev[0]
+        ZB_CUDA(cudaEventRecord(ctx->ev[0], ctx->hs[0]));
+        for (int i = 1; i < zoda_ctx::NHS; i++) ZB_CUDA(cudaStreamWaitEvent(ctx->hs[i], ctx->ev[0], 0));
+        for (uint64_t c = 0; c < nch; c++) {
+            const int b = (int)(c % zoda_ctx::NHS);
+            cudaStream_t st = ctx->hs[b];
+            const uint64_t c0 = c * cw, w = (cols - c0 < cw) ? cols - c0 : cw;
+            uint32_t* din = (uint32_t*)ctx->hin[b].p;
+            uint32_t* dout = (uint32_t*)ctx->hout[b].p;
+            cudaEvent_t* e = ctx->cev[c];
+            ZB_CUDA(cudaEventRecord(e[0], st));
+            ZB_CUDA(cudaMemcpy2DAsync(din, w * 4, h_in + c0, cols * 4, w * 4, k, cudaMemcpyHostToDevice, st));
+            h2d_bytes += (uint64_t)k * w * 4;
+            ZB_CUDA(cudaEventRecord(e[1], st));
+            if (ctx->fault_site == ZODA_FAULT_HOST_CHUNK && ctx->fault_after-- == 0) {
+                ctx->fault_site = 0;
+                set_last_error_text("injected fault: zoda_extend_host chunk launch");
+                return ZODA_ERR_CUDA;
+            }
+            r = ls > 12 ? long_extend(ctx, ls, long_tabs, din, dout, w, st, true)
+                        : launch_extend(ctx, ls, din, dout, w, st, ctx->impl, true);
+            if (r != ZODA_OK) return r;
+            ZB_CUDA(cudaEventRecord(e[2], st));
+            // odd rows 1, 3, .. of the output: a stride of two output rows
+            ZB_CUDA(cudaMemcpy2DAsync(h_out + cols + c0, 2 * cols * 4, dout, w * 4, w * 4, (size_t)k,
                                       cudaMemcpyDeviceToHost, st));
-        ZB_CUDA(cudaEventRecord(e[3], st));
+            d2h_bytes += (uint64_t)k * w * 4;
+            if (c0 >= host_cols) {  // even rows 0, 2, .. of this chunk: the uploaded input, before the buffer is reused
+                ZB_CUDA(cudaMemcpy2DAsync(h_out + c0, 2 * cols * 4, din, w * 4, w * 4, (size_t)k,
+                                          cudaMemcpyDeviceToHost, st));
+                d2h_bytes += (uint64_t)k * w * 4;
+            }
+            ZB_CUDA(cudaEventRecord(e[3], st));
+        }
+        for (int i = 1; i < zoda_ctx::NHS; i++) {
+            ZB_CUDA(cudaEventRecord(ctx->ev[1], ctx->hs[i]));
+            ZB_CUDA(cudaStreamWaitEvent(ctx->hs[0], ctx->ev[1], 0));
+        }
+        ZB_CUDA(cudaEventRecord(ctx->ev[3], ctx->hs[0]));
+        ZB_CUDA(cudaEventSynchronize(ctx->ev[3]));
+        return ZODA_OK;
+    };
+    s = pipeline();
+    if (s != ZODA_OK) {
+        for (int i = 0; i < zoda_ctx::NHS; i++)
+            if (ctx->hs[i]) cudaStreamSynchronize(ctx->hs[i]);  // drain; the first failure is what is reported
+        return s;  // `even` joins its host threads on the way out
     }
-    for (int i = 1; i < zoda_ctx::NHS; i++) {
-        ZB_CUDA(cudaEventRecord(ctx->ev[1], ctx->hs[i]));
-        ZB_CUDA(cudaStreamWaitEvent(ctx->hs[0], ctx->ev[1], 0));
-    }
-    ZB_CUDA(cudaEventRecord(ctx->ev[3], ctx->hs[0]));
-    ZB_CUDA(cudaEventSynchronize(ctx->ev[3]));
     even.join();
     if (timing) {
         float h = 0, kk = 0, d = 0, x = 0;
@@ -424,6 +485,8 @@ zoda_status zoda_extend_host(zoda_ctx* ctx, const uint32_t* h_in, uint32_t* h_ou
         timing->d2h_ms = d;
         timing->total_ms =
             std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+        timing->h2d_bytes = h2d_bytes;
+        timing->d2h_bytes = d2h_bytes;
     }
     return ZODA_OK;
 }

@@ -12,7 +12,8 @@
 // Candidates: the direct-load kernel with radix-16 or radix-8 levels (512 or
 // 1024 threads), either radix schedule and either tile order; the TMA-staged kernel (sides >= 32) with radix-16 or radix-8
 // levels (512 or 1024 threads), L2 promotion 256 B or none, either tile order,
-// and the warp-group stagger released late, early or off.
+// and the warp-group stagger released late, early or off; from side 1024, the
+// three four-step passes (fourstep.cu) in four launch shapes.
 #include <algorithm>
 #include <vector>
 
@@ -55,7 +56,7 @@ std::vector<zoda_plan> candidates(int ls) {
     c.push_back(d);
     auto same = [](const zoda_plan& a, const zoda_plan& b) {
         return a.impl == b.impl && a.sched == b.sched && a.l2_promo == b.l2_promo && a.blocked == b.blocked &&
-               a.stagger == b.stagger && a.radix == b.radix;
+               a.stagger == b.stagger && a.radix == b.radix && a.ctas == b.ctas;
     };
     auto add = [&](zoda_plan p) {
         for (const auto& q : c)
@@ -91,6 +92,18 @@ std::vector<zoda_plan> candidates(int ls) {
                         add(p);
                     }
     }
+    if (ls >= FOURSTEP_MIN_LOG)  // three four-step passes, in each launch shape
+        for (const auto& rc : {std::pair<int, int>{16, 1}, {16, 2}, {8, 2}, {8, 4}}) {
+            zoda_plan p = d;
+            p.impl = ZODA_IMPL_FOURSTEP;
+            p.sched = 0;
+            p.l2_promo = 3;
+            p.blocked = 0;
+            p.stagger = 1;
+            p.radix = rc.first;
+            p.ctas = rc.second;
+            add(p);
+        }
     return c;
 }
 

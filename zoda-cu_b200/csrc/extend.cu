@@ -123,8 +123,14 @@ zoda_plan default_plan(int log_s) {
 
 zoda_status check_plan(int log_s, const zoda_plan& p) {
     if (log_s < 0 || log_s > 12) return ZODA_ERR_UNSUPPORTED;
-    if (p.impl != ZODA_IMPL_DIRECT && p.impl != ZODA_IMPL_TMA) return ZODA_ERR_ARG;
+    if (p.impl != ZODA_IMPL_DIRECT && p.impl != ZODA_IMPL_TMA && p.impl != ZODA_IMPL_FOURSTEP) return ZODA_ERR_ARG;
     if (p.impl == ZODA_IMPL_TMA && log_s < 5) return ZODA_ERR_UNSUPPORTED;
+    if (p.impl == ZODA_IMPL_FOURSTEP) {
+        if (log_s < FOURSTEP_MIN_LOG) return ZODA_ERR_UNSUPPORTED;
+        if (p.ctas < 0 || p.ctas > 4 || p.ctas == 3 || (p.radix == 16 && p.ctas == 4) ||
+            (p.radix == 8 && p.ctas <= 1))
+            return ZODA_ERR_ARG;
+    }
     if (p.sched < 0 || p.sched > 1 || p.l2_promo < 0 || p.l2_promo > 3 || p.blocked < 0 || p.blocked > 1 ||
         p.stagger < 0 || p.stagger > 3 || (p.radix != 16 && p.radix != 8))
         return ZODA_ERR_ARG;
@@ -146,6 +152,15 @@ zoda_status launch_plan(const zoda_ctx* ctx, int log_s, const zoda_plan& p, cons
     if (in_rows == 0) in_rows = S;
     if (out_rows == 0) out_rows = 2 * S;
     if (in_rows > S || out_rows > 2 * S || (log_s == 0 && (in_rows != 1 || out_rows != 2))) return ZODA_ERR_ARG;
+    if (p.impl == ZODA_IMPL_FOURSTEP) {
+        // three four-step passes; they keep their intermediate matrices in the odd
+        // output rows, so an output cut short (an encode of fewer rows) takes the
+        // side's default plan instead
+        if (in_rows == S && out_rows == 2 * S)
+            return long_extend(ctx, log_s, ctx->tables.ext4[log_s], in, out, cols, st, odd_only,
+                               fourstep_shape(p.radix, p.ctas));
+        return launch_plan(ctx, log_s, default_plan(log_s), in, out, cols, st, odd_only, in_rows, out_rows);
+    }
     // stagger 1: release after all INTT levels but the last; 2: after the first; 3: right away
     const uint32_t at_code = p.stagger == 2 ? 2u : p.stagger == 3 ? 1u : 0u;
     const uint32_t flags = (p.blocked ? 1u : 0u) | (p.stagger ? 0u : 2u) | (at_code << 2) | (odd_only ? 16u : 0u);
@@ -184,6 +199,7 @@ zoda_status launch_extend(const zoda_ctx* ctx, int log_s, const uint32_t* in, ui
     if (impl == ZODA_IMPL_AUTO && ctx->planned[log_s]) p = ctx->plan[log_s];
     else if (impl == ZODA_IMPL_DIRECT) p.impl = ZODA_IMPL_DIRECT;
     else if (impl == ZODA_IMPL_TMA) p.impl = ZODA_IMPL_TMA;
+    else if (impl == ZODA_IMPL_FOURSTEP && log_s >= FOURSTEP_MIN_LOG) p.impl = ZODA_IMPL_FOURSTEP;
     return launch_plan(ctx, log_s, p, in, out, cols, st, odd_only, in_rows, out_rows);
 }
 

@@ -1,0 +1,288 @@
+// Long-column transforms: the four-step decomposition of a column NTT of length
+// S = N1 * N2 (S up to 2^26) into passes of N1 or N2 points, each on the same
+// register-resident DIF levels as the single-pass kernels (extend.cuh).
+//
+// With input index i = N2*i1 + i2 and output index k = k1 + N1*k2,
+//   X[k1 + N1*k2] = sum_{i2} w_N2^(i2*k2) * [ w_S^(i2*k1) * sum_{i1} x[N2*i1 + i2] * w_N1^(i1*k1) ]
+// so pass A transforms over i1 (rows N2 apart: a "wide" matrix whose row i1 is
+// the N2 consecutive rows N2*i1 .. N2*i1 + N2-1) and multiplies output k1 of
+// wide column i2 by w_S^(i2*k1); pass B transforms over i2 inside block k1 (the
+// N2 consecutive rows N2*k1 + i2) and writes row k1 + N1*k2 in natural order.
+//
+// Every pass reads and writes matrices through a View: element (row r, virtual
+// quad v) sits at base + (v / qpc) * cb_pitch + (v % qpc) * 4 + r * row_pitch,
+// i.e. quads (4 adjacent u32 columns, one 16-byte vector) are grouped into
+// column blocks of qpc quads. Pass A's column block is i2 (row pitch N2*cols,
+// block pitch cols); pass B's is k1 (row pitch cols, block pitch N2*cols).
+//
+// Fused passes run two transforms of the same length with a pointwise factor
+// between them in registers:
+//   * k_step2<.., INV1 = true, INV2 = false>: pass B of an INTT, the factor,
+//     pass A of the following NTT (whose decomposition is (N2, N1), so its
+//     wide column is the INTT's block): a "block" pass;
+//   * k_step2<.., false, true>: pass B of an NTT, the factor, pass A of the
+//     following INTT with the same decomposition: a "strided" pass.
+#pragma once
+#include "extend.cuh"
+
+namespace zb {
+
+constexpr int LOG_TWM = 26;  // master root omega_{2^26}: w_S^e = w_M^(e * M / S)
+constexpr uint32_t TWM_MASK = (1u << LOG_TWM) - 1;
+
+struct View {
+    uint32_t* base;
+    uint64_t row_pitch;  // u32 between rows
+    uint64_t cb_pitch;   // u32 between column blocks
+};
+
+// Factor f(r, cb) = tab[r * rm + cb * cm], a Shoup pair; tab == nullptr: 1.
+struct FTab {
+    const uint2* tab;
+    uint32_t rm, cm;
+};
+
+struct StepArgs {
+    View in, out;
+    View copy;        // base != nullptr: every loaded input row is also stored here, unchanged
+    uint32_t qpc;     // quads per column block
+    uint64_t nquads;  // virtual quads of the pass
+    // an input row whose index r * lim_rm + cb * lim_cm (its row in the
+    // original matrix) is >= in_limit is zero and not read
+    uint32_t in_lim_rm, in_lim_cm;
+    uint64_t in_limit;
+    // an output whose index k * out_lim_rm + cb * out_lim_cm is >= out_limit
+    // is not stored
+    uint32_t out_lim_rm, out_lim_cm;
+    uint64_t out_limit;
+    FTab pre;         // per input row (k_step): a zero factor skips the load
+    FTab mid1, mid2;  // k_step2: factors on the first transform's output k
+    FTab post;        // per output
+    int tw_log;       // > 0: output (k, cb) times omega_{2^tw_log}^(+-cb * k), sign - when tw_inv
+    int tw_inv;
+    int use_scale;  // output times `scale`
+    Tw scale;
+    uint32_t count_from;          // k_step2 with counter: count nonzero first-transform outputs k >= count_from
+    unsigned long long* counter;  // or nullptr
+};
+
+__device__ __forceinline__ Tw ftab_at(const FTab& f, uint32_t r, uint32_t cb) {
+    const uint2 u = __ldg(f.tab + (r * f.rm + cb * f.cm));
+    return Tw{u.x, u.y};
+}
+
+// x times omega_{2^tw_log}^(+-e) for e < 2^tw_log, from the two-level table:
+// E = e * 2^(26 - tw_log); w_M^E = tw_hi[E >> 13] * tw_lo[E & 8191], where
+// tw_hi = omega_8192^j (the context's table) and tw_lo = omega_{2^26}^j.
+__device__ __forceinline__ void mul_tw2d(V4& x, uint32_t e, int tw_log, bool inv, const Tw* __restrict__ tw_hi,
+                                         const Tw* __restrict__ tw_lo) {
+    uint32_t E = (e << (LOG_TWM - tw_log)) & TWM_MASK;
+    if (inv) E = (0u - E) & TWM_MASK;
+    const uint32_t hi = E >> 13, lo = E & 8191u;
+    if (hi) {
+        const uint2 u = __ldg(reinterpret_cast<const uint2*>(tw_hi) + hi);
+        mul4(x, Tw{u.x, u.y});
+    }
+    if (lo) {
+        const uint2 u = __ldg(reinterpret_cast<const uint2*>(tw_lo) + lo);
+        mul4(x, Tw{u.x, u.y});
+    }
+}
+
+// Quad v's column block and the offset of its 4 columns inside the block.
+struct QuadPos {
+    uint32_t cb, qi;
+    bool active;
+    __device__ __forceinline__ QuadPos(uint64_t v, const StepArgs& a) {
+        active = v < a.nquads;
+        const uint32_t vv = active ? (uint32_t)v : 0u;
+        cb = vv / a.qpc;
+        qi = vv - cb * a.qpc;
+    }
+};
+
+// Level 0 input: rows t + L0*j of the thread's quad, pre-factors applied, rows
+// past the limit (or with a zero factor) as zeros.
+template <class PL>
+__device__ __forceinline__ void step_load(V4* v, const StepArgs& a, const QuadPos& p, int t) {
+    constexpr int R0 = 1 << PL::lr(0);
+    constexpr int L0 = PL::S / R0;
+    const uint32_t* src = a.in.base + (uint64_t)p.cb * a.in.cb_pitch + 4ull * p.qi;
+#pragma unroll
+    for (int j = 0; j < R0; j++) {
+        const uint32_t row = (uint32_t)t + (uint32_t)L0 * j;
+        bool ld = p.active && (uint64_t)row * a.in_lim_rm + (uint64_t)p.cb * a.in_lim_cm < a.in_limit;
+        Tw f{1u, 0u};
+        if (a.pre.tab && ld) {
+            f = ftab_at(a.pre, row, p.cb);
+            ld = f.w != 0;
+        }
+        if (ld) {
+            v[j] = ldg_stream_v4(src + (uint64_t)row * a.in.row_pitch);
+            if (a.copy.base)
+                stg_stream_v4(a.copy.base + (uint64_t)p.cb * a.copy.cb_pitch + 4ull * p.qi +
+                                  (uint64_t)row * a.copy.row_pitch,
+                              v[j]);
+            if (a.pre.tab) mul4(v[j], f);
+        } else {
+            v[j] = V4{{0, 0, 0, 0}};
+        }
+    }
+}
+
+// Output k of the thread's quad: post factors, then the store (if in range).
+__device__ __forceinline__ void step_store(V4 x, const StepArgs& a, const QuadPos& p, uint32_t k,
+                                           const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo) {
+    if (!p.active || (uint64_t)k * a.out_lim_rm + (uint64_t)p.cb * a.out_lim_cm >= a.out_limit) return;
+    if (a.post.tab) mul4(x, ftab_at(a.post, k, p.cb));
+    if (a.tw_log) mul_tw2d(x, p.cb * k, a.tw_log, a.tw_inv, tw, tw_lo);
+    if (a.use_scale) mul4(x, a.scale);
+    stg_stream_v4(a.out.base + (uint64_t)p.cb * a.out.cb_pitch + 4ull * p.qi + (uint64_t)k * a.out.row_pitch, x);
+}
+
+// Launch shapes of the passes: level radix 2^LEPT, THREADS per CTA, MINB CTAs
+// resident per SM (MINB > 1 lets one CTA load its tile while another computes,
+// which the single-CTA shape cannot do: its loads go straight to registers).
+//   0: radix 16 / 512 threads (radix 8 / 1024 from 512 points), one CTA per SM
+//   1: radix 16, 256 threads, 2 per SM      2: radix 8, 512 threads, 2 per SM
+//   3: radix 8, 256 threads, 4 per SM       (1..3: transforms of 32..256 points)
+constexpr int STEP_SHAPES = 4;
+constexpr int STEP_SHAPE_MAX_LOG = 8;
+template <int LOG_N, int SHAPE>
+struct StepShape {
+    static constexpr int LEPT = SHAPE == 0 ? (LOG_N >= 9 ? 3 : 4) : SHAPE == 1 ? 4 : 3;
+    static constexpr int THREADS = SHAPE == 0 ? (LOG_N >= 9 ? 1024 : 512) : SHAPE == 2 ? 512 : 256;
+    static constexpr int MINB = SHAPE == 0 ? 1 : SHAPE == 3 ? 4 : 2;
+    using PL = ExtPlan<LOG_N, 0, LEPT, THREADS>;
+};
+
+// One transform of N = 2^LOG_N points per virtual quad (INV: inverse roots,
+// unscaled), tiles of Q4 consecutive quads dealt round-robin.
+template <int LOG_N, bool INV, int SHAPE>
+__global__ void __launch_bounds__(StepShape<LOG_N, SHAPE>::THREADS, StepShape<LOG_N, SHAPE>::MINB)
+    k_step(const StepArgs a, uint64_t ntiles, const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo) {
+    using PL = typename StepShape<LOG_N, SHAPE>::PL;
+    extern __shared__ uint4 sm[];
+    const int tid = threadIdx.x;
+    const int q = tid % PL::Q4;
+    const int t = tid / PL::Q4;
+    V4 v[PL::EPT];
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const QuadPos p(tile * PL::Q4 + q, a);
+        step_load<PL>(v, a, p, t);
+        dif_levels<PL, 0, INV>(v, sm, t, q, tw);
+        using LV = Level<PL, PL::lr(PL::NLEV - 1), PL::pre(PL::NLEV - 1)>;
+#pragma unroll
+        for (int g = 0; g < LV::G; g++) {
+            const uint32_t blk = LV::gid(g, t);
+#pragma unroll
+            for (int r = 0; r < LV::R; r++) {
+                const uint32_t k = digit_rev<PL, false>((blk << PL::lr(PL::NLEV - 1)) +
+                                                        (uint32_t)bitrev(r, PL::lr(PL::NLEV - 1)));
+                step_store(v[g * LV::R + r], a, p, k, tw, tw_lo);
+            }
+        }
+    }
+}
+
+// The second transform's levels 1 .. NLEV-1 (mirrored radices, as ntt_levels in
+// extend.cuh, with either root direction); the last level stores every output.
+template <class PL, int l, bool INV2>
+__device__ __forceinline__ void step2_levels(V4* v, uint4* sm, int t, int q, const Tw* tw, const Tw* tw_lo,
+                                             const StepArgs& a, const QuadPos& p) {
+    using LV = Level<PL, PL::nlr(l), PL::npre(l)>;
+    if constexpr (l > 0) LV::read(v, sm, t, q);
+    LV::template dft<INV2>(v);
+    if constexpr (l < PL::NLEV - 1) {
+        LV::template twiddle_write<INV2>(v, sm, t, q, tw);
+        __syncthreads();
+        step2_levels<PL, l + 1, INV2>(v, sm, t, q, tw, tw_lo, a, p);
+    } else {
+#pragma unroll
+        for (int g = 0; g < LV::G; g++) {
+            const uint32_t blk = LV::gid(g, t);
+#pragma unroll
+            for (int r = 0; r < LV::R; r++) {
+                const uint32_t k = digit_rev<PL, true>((blk << PL::nlr(l)) + (uint32_t)bitrev(r, PL::nlr(l)));
+                step_store(v[g * LV::R + r], a, p, k, tw, tw_lo);
+            }
+        }
+    }
+}
+
+// Two transforms of N = 2^LOG_N points per virtual quad with a factor between
+// them: out = T2( mid(k) * T1(pre * in)(k) ), T1 with roots w^-1 when INV1,
+// T2 with w^-1 when INV2, both unscaled. mid(k, cb) = mid1(k, cb) * mid2(k, cb).
+// With a counter, the nonzero outputs k >= count_from of T1 (before mid) are
+// counted (the decoder's consistency check).
+template <int LOG_N, bool INV1, bool INV2, int SHAPE>
+__global__ void __launch_bounds__(StepShape<LOG_N, SHAPE>::THREADS, StepShape<LOG_N, SHAPE>::MINB)
+    k_step2(const StepArgs a, uint64_t ntiles, const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo) {
+    using PL = typename StepShape<LOG_N, SHAPE>::PL;
+    extern __shared__ uint4 sm[];
+    const int tid = threadIdx.x;
+    const int q = tid % PL::Q4;
+    const int t = tid / PL::Q4;
+    unsigned long long cnt = 0;
+    V4 v[PL::EPT];
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const QuadPos p(tile * PL::Q4 + q, a);
+        step_load<PL>(v, a, p, t);
+        dif_levels<PL, 0, INV1>(v, sm, t, q, tw);
+        // T1's last level: group g (block b = g*TPQ + t) holds outputs c0 + (S/R)*j at
+        // v[g*R + bitrev(j)]; T2's first level (radix R over stride S/R) wants them in
+        // natural j order as its group n1 = c0, so no exchange sits between the two.
+        constexpr int LR = PL::lr(PL::NLEV - 1);
+        constexpr int R = 1 << LR;
+        constexpr int G = PL::EPT / R;
+        constexpr int SH = PL::LOG_S - LR;
+        uint32_t c0[G];
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            const uint32_t b = (uint32_t)(g * PL::TPQ + t);
+            c0[g] = digit_rev<PL, false>(b << LR);
+            V4 y[R];
+#pragma unroll
+            for (int j = 0; j < R; j++) {
+                y[j] = v[g * R + bitrev(j, LR)];
+                const uint32_t k = c0[g] + ((uint32_t)j << SH);
+                if (a.counter && p.active && k >= a.count_from)
+#pragma unroll
+                    for (int e = 0; e < 4; e++) cnt += y[j].c[e] != 0;
+                if (a.mid1.tab) mul4(y[j], ftab_at(a.mid1, k, p.cb));
+                if (a.mid2.tab) mul4(y[j], ftab_at(a.mid2, k, p.cb));
+            }
+#pragma unroll
+            for (int j = 0; j < R; j++) v[g * R + j] = y[j];
+        }
+        // T2 level 0: radix R over stride S/R, one block; group n1 = c0
+#pragma unroll
+        for (int g = 0; g < G; g++) dft_dif<LR, INV2>(v + g * R);
+        if constexpr (PL::NLEV > 1) {
+            __syncthreads();  // every thread finished reading T1's last level
+#pragma unroll
+            for (int g = 0; g < G; g++) {
+#pragma unroll
+                for (int r = 0; r < R; r++) {
+                    const int k2 = bitrev(r, LR);
+                    V4 x = v[g * R + r];
+                    if (k2 != 0) mul4(x, tw_at<INV2>(tw, c0[g] * (uint32_t)k2, PL::LOG_S));
+                    sm[(size_t)(c0[g] + ((uint32_t)k2 << SH)) * PL::Q4 + q] =
+                        make_uint4(x.c[0], x.c[1], x.c[2], x.c[3]);
+                }
+            }
+            __syncthreads();
+            step2_levels<PL, 1, INV2>(v, sm, t, q, tw, tw_lo, a, p);
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; r++) step_store(v[r], a, p, (uint32_t)bitrev(r, LR), tw, tw_lo);
+        }
+    }
+    if (a.counter) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xFFFFFFFFu, cnt, o);
+        if ((tid & 31) == 0 && cnt) atomicAdd(a.counter, cnt);
+    }
+}
+
+}  // namespace zb

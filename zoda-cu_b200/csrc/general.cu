@@ -386,6 +386,7 @@ zoda_status encode_general(zoda_ctx* ctx, const uint32_t* in, uint32_t* out, uin
     ZB_CUDA(cudaMemcpy2DAsync(out, R * rb, in, rb, rb, mdata, cudaMemcpyDeviceToDevice, st));
     if (m0 > mdata) ZB_CUDA(cudaMemset2DAsync(out + R * mdata * cols, R * rb, 0, rb, m0 - mdata, st));
     if (R == 1) return ZODA_OK;
+    if (lp > 12) return long_encode(ctx, in, out, k, n, cols, st);  // no column fits one pass
     if (P_ == 1) {  // every coset row is the single data row
         for (uint64_t c = 1; c < R && c < rows_out; c++) {
             const uint32_t mc = (uint32_t)((rows_out - c + R - 1) / R);
@@ -456,13 +457,13 @@ zoda_status zoda_encode_device(zoda_ctx* ctx, const uint32_t* d_in, uint32_t* d_
     const char* b = (const char*)d_out;
     if (cols && a < b + rows_out * cols * 4 && b < a + (uint64_t)k * cols * 4) return ZODA_ERR_ARG;  // overlap
     if (next_pow2_64(k) > zoda_max_side() || rows_out > (1ull << 27)) {
-        set_last_error_text("encode supports next_pow2(k) <= 4096 and k + n <= 2^27");
+        set_last_error_text("encode supports next_pow2(k) <= 2^26 and k + n <= 2^27");
         return ZODA_ERR_UNSUPPORTED;
     }
     if (n == k && log2_exact64(k) >= 0) return zoda_extend_device(ctx, d_in, d_out, k, cols, stream);
     if (cols == 0) return ZODA_OK;
     const uint64_t P_ = next_pow2_64(k), N = next_pow2_64(rows_out);
-    if (N == 2 * P_ && P_ >= 2) {
+    if (N == 2 * P_ && P_ >= 2 && P_ <= 4096) {
         // n_kn = 2 n_k: the fused kernels, reading zeros past row k and cutting
         // the output after row k+n
         ZB_CUDA(cudaSetDevice(ctx->device));
@@ -485,8 +486,8 @@ zoda_status zoda_recover_device(zoda_ctx* ctx, const uint32_t* d_code, const uin
     if (((uintptr_t)d_code | (uintptr_t)d_data) & 15) return ZODA_ERR_ARG;
     const int lk = log2_exact64(k);
     if (lk < 0) return ZODA_ERR_ARG;
-    if (lk > 12) {
-        set_last_error_text("the decoder covers k <= 4096 (codewords of up to 8192 rows)");
+    if (lk + 1 > LONG_RECOVER_MAX_LOG) {
+        set_last_error_text("the decoder covers k <= 131072 (codewords of up to 2^18 rows)");
         return ZODA_ERR_UNSUPPORTED;
     }
     const uint32_t N = 2 * k;
@@ -528,19 +529,31 @@ zoda_status zoda_recover_device(zoda_ctx* ctx, const uint32_t* d_code, const uin
     const uint32_t wn = root_of_unity(ln);
     for (uint32_t j = 0, x = 1; j < N; j++, x = mulmod_c(x, wn))
         if (!have[j]) er.push_back(x);
-    if ((s = ctx->gen_tab.ensure((size_t)4 * N * sizeof(uint2))) != ZODA_OK) return finish(s);
+    // gen_small: the erased roots, then the mismatch counter
     if ((s = ctx->gen_small.ensure(std::max<size_t>(1, er.size()) * 4 + 64)) != ZODA_OK) return finish(s);
-    uint2* T = (uint2*)ctx->gen_tab.p;
-    uint2 *zk = T, *izh = T + N, *mid_a = T + 2 * N, *mid_b = T + 3 * N;
     uint32_t* d_er = (uint32_t*)ctx->gen_small.p;
     unsigned long long* d_cnt = (unsigned long long*)((char*)ctx->gen_small.p + ((er.size() * 4 + 15) / 16) * 16);
+    if (mismatch) ZB_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), st));
+    if (ln > 13) {  // above 8192 points: the four transforms as five four-step passes (fourstep.cu)
+        if ((s = long_recover(ctx, d_code, er, k, cols, d_data, mismatch ? d_cnt : nullptr, st)) != ZODA_OK)
+            return finish(s);
+        if (mismatch) {
+            unsigned long long h = 0;
+            ZB_CUDA(cudaMemcpyAsync(&h, d_cnt, sizeof h, cudaMemcpyDeviceToHost, st));
+            ZB_CUDA(cudaStreamSynchronize(st));
+            *mismatch = h;
+        }
+        return finish(ZODA_OK);
+    }
+    if ((s = ctx->gen_tab.ensure((size_t)4 * N * sizeof(uint2))) != ZODA_OK) return finish(s);
+    uint2* T = (uint2*)ctx->gen_tab.p;
+    uint2 *zk = T, *izh = T + N, *mid_a = T + 2 * N, *mid_b = T + 3 * N;
     if (!er.empty())
         ZB_CUDA(cudaMemcpyAsync(d_er, er.data(), er.size() * 4, cudaMemcpyHostToDevice, st));
     const uint32_t ninv = powmod_c(N, P - 2);
     k_erasure_tables<<<(N + 127) / 128, 128, 0, st>>>(d_er, (uint32_t)er.size(), ln, ctx->tables.tw, k, ninv, zk,
                                                       izh, mid_a, mid_b);
     ZB_CUDA(cudaGetLastError());
-    if (mismatch) ZB_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), st));
     const uint64_t w0 = chunk_cols(cols, N);
     if ((s = ctx->gen_a.ensure((uint64_t)N * w0 * 4)) != ZODA_OK) return finish(s);
     uint32_t* A = (uint32_t*)ctx->gen_a.p;

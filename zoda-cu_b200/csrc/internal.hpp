@@ -66,9 +66,13 @@ struct DevBuf {
 //   twist[S + i]     = omega_2S^i * S^-1, i in [0, S), for S = 1 .. 4096
 struct Tables {
     Tw* tw = nullptr;
+    Tw* tw_lo = nullptr;  // omega_{2^26}^j, j in [0, 8192): with tw, every 2^26-th root of unity
     Tw* twist = nullptr;
     // per-side level tables of the TMA-staged kernels (log2 side 5..12), one buffer
     Tw* side = nullptr;
+    // factor tables of the four-step extension plan for log2 side 10..12 (in the
+    // context's coset table map; built at creation so launches need no lock)
+    const uint2* ext4[13] = {};
     // [log_s][radix 16, radix 8][intt0, intt1, intt2, ntt0, ntt1, ntt2, end] entry offsets
     size_t side_off[13][2][8] = {};
 };
@@ -93,6 +97,8 @@ struct zoda_ctx {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t cev[MAX_CHUNKS][4] = {};
     std::mutex mu;  // serialises host calls on one context
+    // armed fault site (zoda_ctx_inject_fault) and the passes left before it fires
+    uint32_t fault_site = 0, fault_after = 0;
     // encode of any (k, n) and erasure decoder (general.cu): two column-chunk
     // scratch matrices, per-pattern tables, coset twist tables keyed by
     // (log2 n_k, log2 n_kn), and an event after each call's last use of them
@@ -133,4 +139,34 @@ void general_release(zoda_ctx* ctx);
 zoda_status rlc_init_attributes();
 // Frees the RLC consumers' scratch.
 void rlc_release(zoda_ctx* ctx);
+
+// Long columns (fourstep.cu): transforms of 2^13 .. 2^26 points in four-step passes.
+constexpr int LONG_MIN_LOG = 13, LONG_MAX_LOG = 26;
+// The decoder's erasure-pattern tables cost O(2k * erasures), so it stops at
+// codewords of 2^18 rows (k = 131072).
+constexpr int LONG_RECOVER_MAX_LOG = 18;
+// Legacy layout: B = [2^L][w4] (polynomials in columns) -> natural-order
+// transform in A ([2^L][w4]); B is overwritten; inverse roots and `scale` when inv.
+zoda_status long_cols_ntt(const zoda_ctx* ctx, uint32_t* B, uint32_t* A, int L, uint64_t w4, bool inv, Tw scale,
+                          cudaStream_t st);
+// The coset factor tables of the long encode over 2^ln points with n_k = 2^L (built
+// once, kept in ctx->coset_tabs: call it holding ctx->mu).
+zoda_status coset_mid_tables(zoda_ctx* ctx, int L, int ln, const uint2** tabs);
+// Extension of a 2^L square (12 <= L <= 26) in three passes, the odd output rows as
+// scratch; odd_only: out is the compact [S][cols] odd rows (the even rows are the input).
+// tabs = coset_mid_tables(ctx, L, L + 1).
+// shape: the launch shape of the passes (fourstep.cuh, StepShape).
+zoda_status long_extend(const zoda_ctx* ctx, int L, const uint2* tabs, const uint32_t* in, uint32_t* out,
+                        uint64_t cols, cudaStream_t st, bool odd_only = false, int shape = 0);
+// The four-step launch shape of a plan's (radix, ctas).
+int fourstep_shape(int radix, int ctas);
+// Smallest side (log2) the four-step plan covers.
+constexpr int FOURSTEP_MIN_LOG = 10;
+// Cosets c >= 1 of the encode of k data rows with n parity rows, n_k = next_pow2(k)
+// in [2^13, 2^26], on the context's scratch (the caller holds ctx->mu and copies coset 0).
+zoda_status long_encode(zoda_ctx* ctx, const uint32_t* in, uint32_t* out, uint32_t k, uint32_t n, uint64_t cols,
+                        cudaStream_t st);
+// k-of-2k recovery for 2k = 2^L, LONG_MIN_LOG < L <= LONG_RECOVER_MAX_LOG (the caller holds ctx->mu).
+zoda_status long_recover(zoda_ctx* ctx, const uint32_t* d_code, const std::vector<uint32_t>& erased_roots,
+                         uint32_t k, uint64_t cols, uint32_t* d_data, unsigned long long* d_cnt, cudaStream_t st);
 }  // namespace zb

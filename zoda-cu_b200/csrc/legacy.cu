@@ -24,24 +24,35 @@ namespace zb {
 
 namespace {
 
-// out[c][r] = in[r][c] for an R x Cn u32 matrix (both dense).
-__global__ void k_transpose(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_t R, uint32_t Cn) {
+// out[c][r] = in[g(r)][c] for an R x Cn u32 matrix (both dense), where
+// g(r) = r, or (r * gmul) mod R when gmul != 1 (R a power of two: the output
+// permutation of a caller's root table). The row tiles are walked with a grid
+// stride in y, so any R fits the 65535-block limit of gridDim.y (R reaches
+// 2^24 polynomials per chunk at n = 2).
+__global__ void k_transpose(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_t R, uint32_t Cn,
+                            uint32_t gmul) {
     __shared__ uint32_t tile[32][33];
-    const uint32_t c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
-    for (uint32_t i = threadIdx.y; i < 32; i += blockDim.y) {
-        const uint32_t r = r0 + i, c = c0 + threadIdx.x;
-        if (r < R && c < Cn) tile[i][threadIdx.x] = in[(size_t)r * Cn + c];
-    }
-    __syncthreads();
-    for (uint32_t i = threadIdx.y; i < 32; i += blockDim.y) {
-        const uint32_t c = c0 + i, r = r0 + threadIdx.x;
-        if (r < R && c < Cn) out[(size_t)c * R + r] = tile[threadIdx.x][i];
+    const uint32_t c0 = blockIdx.x * 32;
+    for (uint32_t r0 = blockIdx.y * 32; r0 < R; r0 += gridDim.y * 32) {
+        for (uint32_t i = threadIdx.y; i < 32; i += blockDim.y) {
+            const uint32_t r = r0 + i, c = c0 + threadIdx.x;
+            const uint32_t g = gmul == 1 ? r : (r * gmul) & (R - 1);
+            if (r < R && c < Cn) tile[i][threadIdx.x] = in[(size_t)g * Cn + c];
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.y; i < 32; i += blockDim.y) {
+            const uint32_t c = c0 + i, r = r0 + threadIdx.x;
+            if (r < R && c < Cn) out[(size_t)c * R + r] = tile[threadIdx.x][i];
+        }
+        __syncthreads();  // the tile is rewritten by the next row tile
     }
 }
 
-zoda_status transpose(const uint32_t* in, uint32_t* out, uint32_t R, uint32_t Cn, cudaStream_t st) {
-    dim3 grid((Cn + 31) / 32, (R + 31) / 32), block(32, 8);
-    k_transpose<<<grid, block, 0, st>>>(in, out, R, Cn);
+zoda_status transpose(const uint32_t* in, uint32_t* out, uint32_t R, uint32_t Cn, cudaStream_t st,
+                      uint32_t gmul = 1) {
+    const uint32_t gy = (R + 31) / 32;
+    dim3 grid((Cn + 31) / 32, gy < 65535u ? gy : 65535u), block(32, 8);
+    k_transpose<<<grid, block, 0, st>>>(in, out, R, Cn, gmul);
     ZB_CUDA(cudaGetLastError());
     return ZODA_OK;
 }
@@ -50,11 +61,9 @@ template <int LOG_N, bool INV>
 zoda_status colntt_t(const zoda_ctx* ctx, const uint32_t* in, uint32_t* out, uint64_t cols, Tw scale, uint32_t a,
                      cudaStream_t st) {
     using PL = ExtPlan<LOG_N>;
-    static bool attr = false;  // guarded by the legacy mutex
-    if (!attr && PL::SMEM > 0) {
+    // per call: the attribute belongs to the current device, and calls may come on any device
+    if (PL::SMEM > 0)
         ZB_CUDA(cudaFuncSetAttribute(k_colntt<LOG_N, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PL::SMEM));
-        attr = true;
-    }
     const uint64_t ntiles = (cols + PL::C - 1) / PL::C;
     const uint64_t grid = ntiles < (uint64_t)ctx->sm_count ? ntiles : (uint64_t)ctx->sm_count;
     k_colntt<LOG_N, INV><<<(unsigned)grid, PL::THREADS, PL::SMEM, st>>>(in, out, cols, ntiles, ctx->tables.tw, scale, a);
@@ -150,7 +159,16 @@ zoda_status legacy_run(uint32_t* values, const uint32_t* roots, uint32_t n, uint
     uint32_t a_inv = 0;
     if (!check_roots(S, roots, n, &a_inv)) return ZODA_ERR_ARG;
     if (n == 1) return ZODA_OK;  // a length-1 transform (and its 1^-1 scale) is the identity
-    if (L > 12) return ZODA_ERR_UNSUPPORTED;
+    if (L > LONG_MAX_LOG) {
+        set_last_error_text("cuda_ntt/cuda_intt: n above 2^26 is not supported");
+        return ZODA_ERR_UNSUPPORTED;
+    }
+    // above 4096 points: four-step passes in natural order, and the caller's
+    // root w = omega^a applied when transposing back: X_w[j] = X_omega[a * j]
+    const bool long_n = L > 12;
+    uint32_t a_fwd = a_inv;  // a = (a^-1)^-1 mod n, by Newton's iteration mod 2^32
+    for (int i = 0; i < 5; i++) a_fwd *= 2u - a_inv * a_fwd;
+    a_fwd &= n - 1;
     if (!S.ctx) {
         zoda_status s = zoda_ctx_create(dev, &S.ctx);
         if (s != ZODA_OK) return s;
@@ -177,9 +195,15 @@ zoda_status legacy_run(uint32_t* values, const uint32_t* roots, uint32_t n, uint
         ZB_CUDA(cudaMemcpy2DAsync(A, per_poly, host, (size_t)stride * 4, per_poly, w, cudaMemcpyHostToDevice, st));
         if (w4 != w) ZB_CUDA(cudaMemsetAsync(A + w * n, 0, (w4 - w) * per_poly, st));
         if ((s = transpose(A, B, (uint32_t)w4, n, st)) != ZODA_OK) return s;  // B = [n][w4]
-        s = inverse ? colntt<true>(ctx, L, B, A, w4, scale, a_inv, st) : colntt<false>(ctx, L, B, A, w4, scale, a_inv, st);
-        if (s != ZODA_OK) return s;
-        if ((s = transpose(A, B, n, (uint32_t)w4, st)) != ZODA_OK) return s;  // B = [w4][n]
+        if (long_n) {
+            if ((s = long_cols_ntt(ctx, B, A, L, w4, inverse, scale, st)) != ZODA_OK) return s;
+            if ((s = transpose(A, B, n, (uint32_t)w4, st, a_fwd)) != ZODA_OK) return s;  // B = [w4][n], permuted
+        } else {
+            s = inverse ? colntt<true>(ctx, L, B, A, w4, scale, a_inv, st)
+                        : colntt<false>(ctx, L, B, A, w4, scale, a_inv, st);
+            if (s != ZODA_OK) return s;
+            if ((s = transpose(A, B, n, (uint32_t)w4, st)) != ZODA_OK) return s;  // B = [w4][n]
+        }
         ZB_CUDA(cudaMemcpy2DAsync(host, (size_t)stride * 4, B, per_poly, per_poly, w, cudaMemcpyDeviceToHost, st));
     }
     ZB_CUDA(cudaStreamSynchronize(st));

@@ -40,20 +40,31 @@ struct NoallocDevice {
 std::mutex g_noalloc_mu;
 std::map<int, NoallocDevice> g_noalloc_dev;
 
-// out[c * ld_out + r] = in[r * ld_in + c] for r < R, c < Cn.
+// out[c * ld_out + r] = in[r * ld_in + c] for r < R, c < Cn. Row tiles are
+// walked with a grid stride in y: R reaches 2^21 polynomials at n = 2, more
+// 32-row tiles than gridDim.y may hold (65535).
 __global__ void k_noalloc_transpose(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_t R,
                                     uint32_t Cn, uint64_t ld_in, uint64_t ld_out) {
     __shared__ uint32_t tile[32][33];
-    const uint32_t c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
-    for (uint32_t i = threadIdx.y; i < 32; i += blockDim.y) {
-        const uint32_t r = r0 + i, c = c0 + threadIdx.x;
-        if (r < R && c < Cn) tile[i][threadIdx.x] = in[r * ld_in + c];
+    const uint32_t c0 = blockIdx.x * 32;
+    for (uint32_t r0 = blockIdx.y * 32; r0 < R; r0 += gridDim.y * 32) {
+        for (uint32_t i = threadIdx.y; i < 32; i += blockDim.y) {
+            const uint32_t r = r0 + i, c = c0 + threadIdx.x;
+            if (r < R && c < Cn) tile[i][threadIdx.x] = in[r * ld_in + c];
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.y; i < 32; i += blockDim.y) {
+            const uint32_t c = c0 + i, r = r0 + threadIdx.x;
+            if (r < R && c < Cn) out[c * ld_out + r] = tile[threadIdx.x][i];
+        }
+        __syncthreads();  // the next row tile reuses the tile buffer
     }
-    __syncthreads();
-    for (uint32_t i = threadIdx.y; i < 32; i += blockDim.y) {
-        const uint32_t c = c0 + i, r = r0 + threadIdx.x;
-        if (r < R && c < Cn) out[c * ld_out + r] = tile[threadIdx.x][i];
-    }
+}
+
+// Grid of a k_noalloc_transpose launch over R x Cn: Cn on x, R on y (capped).
+dim3 noalloc_transpose_grid(uint32_t R, uint32_t Cn) {
+    const uint32_t gy = (R + 31) / 32;
+    return dim3((Cn + 31) / 32, gy < 65535u ? gy : 65535u);
 }
 
 template <int LOG_N, bool INV>
@@ -169,14 +180,12 @@ extern "C" zoda_status zoda_ntt_device_noalloc(const uint32_t* d_in, uint32_t* d
     // columns (polys .. polys4) hold whatever an earlier call left; their
     // results are never copied out, so nothing needs clearing.
     dim3 block(32, 8);
-    k_noalloc_transpose<<<dim3((n + 31) / 32, (polys + 31) / 32), block, 0, st>>>(d_in, d.scratch, polys, n, n,
-                                                                                  polys4);
+    k_noalloc_transpose<<<noalloc_transpose_grid(polys, n), block, 0, st>>>(d_in, d.scratch, polys, n, n, polys4);
     ZB_CUDA(cudaGetLastError());
     s = inverse ? noalloc_colntt<true>(d, log_n, d.scratch, polys4, scale, st)
                 : noalloc_colntt<false>(d, log_n, d.scratch, polys4, scale, st);
     if (s != ZODA_OK) return s;
-    k_noalloc_transpose<<<dim3((polys + 31) / 32, (n + 31) / 32), block, 0, st>>>(d.scratch, d_out, n, polys,
-                                                                                  polys4, n);
+    k_noalloc_transpose<<<noalloc_transpose_grid(n, polys), block, 0, st>>>(d.scratch, d_out, n, polys, polys4, n);
     ZB_CUDA(cudaGetLastError());
     return ZODA_OK;
 }

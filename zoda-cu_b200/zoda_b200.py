@@ -38,7 +38,7 @@ EXPORTS = [
     "zoda_server_release", "zoda_server_cancel", "zoda_server_get_stats", "zoda_server_destroy",
     "zoda_encode_device", "zoda_recover_device", "zoda_autotune", "zoda_plan_get", "zoda_plan_set",
     "zoda_plan_clear", "zoda_data_root_host", "zoda_rlc_coefficients_device", "zoda_rlc_rows_device",
-    "zoda_rlc_check_device",
+    "zoda_rlc_check_device", "zoda_ctx_inject_fault",
 ]
 
 _lib = None
@@ -74,16 +74,17 @@ class ZodaServerStats(ctypes.Structure):
 
 class ZodaTiming(ctypes.Structure):
     _fields_ = [("h2d_ms", ctypes.c_float), ("kernel_ms", ctypes.c_float),
-                ("d2h_ms", ctypes.c_float), ("total_ms", ctypes.c_float)]
+                ("d2h_ms", ctypes.c_float), ("total_ms", ctypes.c_float),
+                ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64)]
 
 
 class ZodaPlan(ctypes.Structure):
     """Per-side launch plan (include/zoda_b200.h, zoda_plan)."""
     _fields_ = [("impl", ctypes.c_int32), ("sched", ctypes.c_int32), ("l2_promo", ctypes.c_int32),
                 ("blocked", ctypes.c_int32), ("stagger", ctypes.c_int32), ("radix", ctypes.c_int32),
-                ("ms", ctypes.c_float)]
-    KEYS = ("impl", "sched", "l2_promo", "blocked", "stagger", "radix", "ms")
-    DEFAULTS = {"radix": 16}
+                ("ms", ctypes.c_float), ("ctas", ctypes.c_int32)]
+    KEYS = ("impl", "sched", "l2_promo", "blocked", "stagger", "radix", "ms", "ctas")
+    DEFAULTS = {"radix": 16, "ctas": 0}
 
     def to_dict(self) -> dict:
         return {k: (round(float(getattr(self, k)), 5) if k == "ms" else int(getattr(self, k))) for k in self.KEYS}
@@ -176,6 +177,8 @@ def load(path: str = LIB_PATH):
                                         ctypes.POINTER(ctypes.c_uint64), vp]
     L.zoda_ntt_device_noalloc.restype = ctypes.c_int
     L.zoda_ntt_device_noalloc.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, vp]
+    L.zoda_ctx_inject_fault.restype = ctypes.c_int
+    L.zoda_ctx_inject_fault.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32]
     L.zoda_extend_host.restype = ctypes.c_int
     L.zoda_extend_host.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(ZodaTiming)]
     del u32p
@@ -317,7 +320,7 @@ class Context:
             self.plan_set(int(side), p)
 
     def set_impl(self, impl: int):
-        """0 = automatic, 1 = direct-load kernel, 2 = TMA-staged kernel."""
+        """0 = automatic, 1 = direct-load kernel, 2 = TMA-staged kernel, 3 = four-step passes."""
         _check(load().zoda_ctx_set_impl(self._h, impl), "zoda_ctx_set_impl")
 
     def check(self):
@@ -328,6 +331,11 @@ class Context:
         """Run a kernel whose barrier wait nothing completes; the next check() raises
         ZODA_ERR_TIMEOUT (and clears the flag)."""
         _check(load().zoda_selftest_bounded_wait(self._h, _stream_handle(stream)), "zoda_selftest_bounded_wait")
+
+    def inject_fault(self, site: int, after: int = 0):
+        """Arm a fault site (zoda_ctx_inject_fault): 1 = a column-chunk launch of
+        extend_host, failing after `after` chunks; 0 disarms."""
+        _check(load().zoda_ctx_inject_fault(self._h, site, after), "zoda_ctx_inject_fault")
 
     def extend_host(self, h_in, h_out, k: int, cols: int) -> ZodaTiming:
         t = ZodaTiming()
