@@ -502,7 +502,10 @@ def time_host_extend(ctx, side: int, steps: int, warmup: int):
     import torch
     cols = side * SHARE_U32
     gen = torch.Generator().manual_seed(99)
-    h_in = torch.randint(0, P, (side, cols), dtype=torch.int64, generator=gen).to(torch.int32).pin_memory()
+    h_in = torch.empty((side, cols), dtype=torch.int32).pin_memory()
+    for r0 in range(0, side, 256):  # seeded uniform in [0, p), in slabs to bound the int64 temporary
+        r1 = min(side, r0 + 256)
+        h_in[r0:r1] = torch.randint(0, P, (r1 - r0, cols), dtype=torch.int64, generator=gen).to(torch.int32)
     h_out = torch.empty((2 * side, cols), dtype=torch.int32).pin_memory()
     for _ in range(warmup):
         ctx.extend_host(h_in, h_out, side, cols)

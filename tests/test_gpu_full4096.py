@@ -3,6 +3,8 @@ validated the way its workload asks: the RLC check of every one of the 8192
 encoded rows (src/benchmarks/utils.rs:225-272, on the device) and a random
 k-of-2k erasure recovery (k = 4096) on a window of columns, plus a CPU
 re-encode of sampled columns (utils.rs:185-218) by the oracle."""
+import hashlib
+
 import numpy as np
 import pytest
 
@@ -14,6 +16,18 @@ pytestmark = pytest.mark.gpu
 P = O.P
 K = 4096
 COLS = K * 128
+
+
+def data_root_streamed(rows) -> str:
+    """compute_data_root (utils.rs:51-59) of a device matrix: SHA-256 over the little-endian
+    row bytes, streamed to the host in slabs of 32 rows."""
+    h = hashlib.sha256()
+    buf = torch.empty((32, rows.shape[1]), dtype=torch.int32).pin_memory()
+    for r0 in range(0, rows.shape[0], 32):
+        n = min(32, rows.shape[0] - r0)
+        buf[:n].copy_(rows[r0:r0 + n])
+        h.update(buf[:n].numpy())
+    return h.hexdigest()
 
 
 @pytest.fixture(scope="module")
@@ -51,7 +65,8 @@ def test_sampled_columns_match_cpu_reencode(square):
 def test_rlc_check_of_every_row(square):
     ctx, d_in, d_out = square
     coeff = torch.empty((COLS, 4), dtype=torch.int32, device="cuda")
-    ctx.rlc_coefficients("full-square-4096", COLS, coeff)
+    # coefficients from the data root of the encoded rows, as the reference derives them
+    ctx.rlc_coefficients(data_root_streamed(d_out), COLS, coeff)
     assert ctx.rlc_check(d_in, d_out, K, K, COLS, coeff) == 0
     # one wrong share in one row is caught (all four limbs of that row)
     d_out[5001, 77] = (int(d_out[5001, 77]) + 1) % P
