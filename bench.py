@@ -308,13 +308,14 @@ def time_long_leg(ctx) -> dict:
     out["cuda_ntt_131072"] = res
     side, cols = 4096, 4096 * SHARE_U32
     shapes = {}
-    for radix, ctas in ((16, 1), (16, 2), (8, 2), (8, 4)):
-        ctx.plan_set(side, {"impl": 3, "sched": 0, "l2_promo": 3, "blocked": 0, "stagger": 1, "radix": radix,
-                            "ctas": ctas})
-        ms, _, check = time_device_extend(ctx, side, 5, 2, 1, verify=(radix, ctas) == (8, 2), cols=cols)
-        shapes[f"radix{radix}_ctas{ctas}"] = {"ms": round(ms / 5, 4),
-                                              "check_mismatches": check["check_mismatches"] if check else None}
-        torch.cuda.empty_cache()
+    for blocked in (0, 1):  # three launches over the square, or one pipelined launch chunk by chunk
+        for radix, ctas in ((16, 1), (16, 2), (8, 2), (8, 4)):
+            ctx.plan_set(side, {"impl": 3, "sched": 0, "l2_promo": 3, "blocked": blocked, "stagger": 1,
+                                "radix": radix, "ctas": ctas})
+            ms, _, check = time_device_extend(ctx, side, 5, 2, 1, verify=(radix, ctas) == (8, 2), cols=cols)
+            shapes[f"{'pipelined' if blocked else 'three_launches'}_radix{radix}_ctas{ctas}"] = {
+                "ms": round(ms / 5, 4), "check_mismatches": check["check_mismatches"] if check else None}
+            torch.cuda.empty_cache()
     ctx.plan_clear()
     out["fourstep_side4096"] = shapes
     return out

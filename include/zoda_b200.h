@@ -113,7 +113,10 @@ typedef struct zoda_plan {
                          or its first level (1)                                        */
     int32_t l2_promo; /* TMA kernel: L2 promotion of tile loads, 0 none, 1 64 B,
                          2 128 B, 3 256 B                                              */
-    int32_t blocked;  /* 0 = CTA i takes tiles i, i + grid, ...; 1 = one contiguous run */
+    int32_t blocked;  /* 0 = CTA i takes tiles i, i + grid, ...; 1 = one contiguous run.
+                         FOURSTEP: 0 = three launches over the whole square; 1 = one
+                         persistent launch that runs the three passes column chunk by
+                         column chunk, so each chunk's intermediate stays in L2      */
     int32_t stagger;  /* TMA kernel: 0 = the two warp-groups run in step; 1, 2, 3 = the
                          second starts once the first begins its last INTT level, its
                          second INTT level, or its first (less apart, more shared code) */

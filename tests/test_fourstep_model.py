@@ -52,8 +52,14 @@ def model_pass(a: dict):
     None), scale, in_lim / out_lim ((rm, cm, limit) or None), copy (View or None),
     count_from (int or None; returns the count)."""
     N, qpc, nq = a["N"], a["qpc"], a["nquads"]
-    v = np.arange(nq * 4)
+    # a["quads"] = (q0, q1): only virtual quads q0 .. q1-1 (one tile); a["qlim"]: quads
+    # at or past it inside a column block are not real (the pipeline's ragged last chunk)
+    q0, q1 = a.get("quads", (0, nq))
+    v = np.arange(q0 * 4, min(q1, nq) * 4)
     cb, ci = (v // 4) // qpc, (v // 4) % qpc * 4 + v % 4
+    if a.get("qlim") is not None:
+        keep = (v // 4) % qpc < a["qlim"]
+        v, cb, ci = v[keep], cb[keep], ci[keep]
     r = np.arange(N)[:, None]
     ia = addr(a["in"], r, cb[None, :], ci[None, :])
     ld = np.ones((N, len(v)), dtype=bool)
@@ -134,6 +140,100 @@ def model_extend(data: np.ndarray) -> np.ndarray:
                     mid1=(cbt, 0, 1), mid2=(kt, 1, 0), tw=(L, 0)))
     strd = View(out, cols, 2 * N2 * cols, 2 * cols)
     model_pass(dict(N=N1, inv=False, **{"in": strd}, out=strd, qpc=qpc, nquads=N2 * qpc))
+    return out.reshape(2 * S, cols).astype(np.uint32)
+
+
+def pipe_geometry(L: int, q4a: int, q4m: int, grid: int, cols: int) -> dict:
+    """fourstep.cu pipe_t: chunk quads, tiles per chunk and pass, chunks, depth."""
+    L1, L2, N1, N2 = split(L)
+    cq = max(q4a, q4m)
+    quads = cols // 4
+    nch = -(-quads // cq)
+    tiles = [N2 * cq // q4a, N1 * cq // q4m, N2 * cq // q4a]
+    per_round = sum(tiles)
+    depth = max(1, -(-(2 * 2 * grid) // per_round))
+    return dict(cq=cq, nch=nch, tiles=tiles, per_round=per_round, depth=depth,
+                last_qlim=quads - (nch - 1) * cq, total=(nch + 2 * depth) * per_round)
+
+
+def pipe_decode(item: int, g: dict):
+    """k_fourstep_pipe's item -> (pass, chunk, tile); chunk None for an empty item."""
+    r, j = divmod(item, g["per_round"])
+    t = g["tiles"]
+    if j < t[0]:
+        ph, c = 0, r
+    elif j < t[0] + t[1]:
+        ph, c, j = 1, r - g["depth"], j - t[0]
+    else:
+        ph, c, j = 2, r - 2 * g["depth"], j - t[0] - t[1]
+    return ph, (c if 0 <= c < g["nch"] else None), j
+
+
+def model_extend_pipelined(data: np.ndarray, q4a: int, q4m: int, grid: int, seed: int) -> np.ndarray:
+    """k_fourstep_pipe: the passes of long_extend as tiles of (chunk, pass), dealt in the
+    kernel's order to `grid` CTAs that each hold one item and the next one drawn, and
+    finished in a random order among those whose dependencies are met (a pass-B or block
+    tile waits for every tile of the chunk's previous pass). Fails on a deadlock, a tile
+    run twice or missed, or a tile run before its dependencies."""
+    S, cols = data.shape
+    L = S.bit_length() - 1
+    L1, L2, N1, N2 = split(L)
+    g = pipe_geometry(L, q4a, q4m, grid, cols)
+    cq = g["cq"]
+    inp = data.astype(np.uint64).ravel()
+    out = np.full(2 * S * cols, 12345, dtype=np.uint64)
+    cbt, kt = coset_mid_tables(L, L + 1)[0]
+    nq = {0: N2 * cq, 1: N1 * cq, 2: N2 * cq}
+
+    def args(ph, c):
+        off = c * 4 * cq
+        qlim = g["last_qlim"] if c == g["nch"] - 1 else cq
+        if ph == 0:
+            return dict(N=N1, inv=True, **{"in": View(inp, off, N2 * cols, cols)},
+                        out=View(out, cols + off, 2 * N2 * cols, 2 * cols), qpc=cq, nquads=nq[0], tw=(L, 1),
+                        copy=View(out, off, 2 * N2 * cols, 2 * cols), qlim=qlim), q4a
+        if ph == 1:
+            blk = View(out, cols + off, 2 * cols, 2 * N2 * cols)
+            return dict(N=N2, inv=True, two=True, **{"in": blk}, out=blk, qpc=cq, nquads=nq[1],
+                        mid1=(cbt, 0, 1), mid2=(kt, 1, 0), tw=(L, 0), qlim=qlim), q4m
+        strd = View(out, cols + off, 2 * N2 * cols, 2 * cols)
+        return dict(N=N1, inv=False, **{"in": strd}, out=strd, qpc=cq, nquads=nq[2], qlim=qlim), q4a
+
+    rng = np.random.default_rng(seed)
+    counter = 0
+    done = {0: np.zeros(g["nch"], int), 1: np.zeros(g["nch"], int)}
+    ran = set()
+
+    def draw():
+        nonlocal counter
+        counter += 1
+        return counter - 1
+
+    ctas = [[draw(), None] for _ in range(grid)]  # [current, drawn next]
+    while True:
+        live = [k for k, (it, _) in enumerate(ctas) if it < g["total"]]
+        if not live:
+            break
+        ready = []
+        for k in live:
+            ph, c, _ = pipe_decode(ctas[k][0], g)
+            if c is None or ph == 0 or done[ph - 1][c] >= g["tiles"][ph - 1]:
+                ready.append(k)
+        assert ready, "deadlock: every CTA waits"
+        k = ready[rng.integers(len(ready))]
+        item = ctas[k][0]
+        ctas[k][1] = draw()
+        ph, c, j = pipe_decode(item, g)
+        if c is not None:
+            assert (ph, c, j) not in ran
+            ran.add((ph, c, j))
+            a, q4 = args(ph, c)
+            a["quads"] = (j * q4, j * q4 + q4)
+            model_pass(a)
+            if ph < 2:
+                done[ph][c] += 1
+        ctas[k] = [ctas[k][1], None]
+    assert len(ran) == g["nch"] * sum(g["tiles"])
     return out.reshape(2 * S, cols).astype(np.uint32)
 
 
@@ -277,3 +377,23 @@ def test_model_recover():
     garbage[known[3], 1] = (int(garbage[known[3], 1]) + 1) % P
     _, cnt = model_recover(garbage, known, k, check=True)
     assert cnt > 0
+
+
+# (L, Q4 of the strided passes, Q4 of the block pass, grid, columns): the kernel's tile
+# widths per launch shape (Q4 = threads / (N / positions per thread)), small grids so
+# that chunks overlap, ragged column counts so the last chunk is partial
+@pytest.mark.parametrize("L,q4a,q4m,grid,cols", [(10, 256, 256, 3, 4 * 256 * 3 + 8), (11, 256, 128, 5, 4 * 256 * 4 + 12),
+                                                 (12, 128, 128, 7, 4 * 128 * 5 + 4), (12, 32, 32, 16, 4 * 32 * 9 + 20),
+                                                 (13, 128, 64, 4, 4 * 128 * 3 + 16)])
+def test_model_pipelined_extension_matches_oracle(L, q4a, q4m, grid, cols):
+    S = 1 << L
+    data = O.seeded_input(S, cols, seed=L + cols)
+    assert np.array_equal(model_extend_pipelined(data, q4a, q4m, grid, seed=L), O.encode_rowmajor(data))
+
+
+def test_pipe_geometry_limits():
+    # the kernel's item counter is 32-bit: the host keeps every draw below 2^31
+    for L, q4a, q4m in ((10, 256, 256), (12, 128, 128), (12, 32, 32), (14, 64, 64)):
+        g = pipe_geometry(L, q4a, q4m, 592, 1 << 26)
+        assert g["total"] + 2 * 592 < 1 << 31
+        assert all(t * q for t, q in zip(g["tiles"], (q4a, q4m, q4a)))

@@ -133,10 +133,11 @@ FOURSTEP_SHAPES = [(16, 1), (16, 2), (8, 2), (8, 4)]
 
 @pytest.mark.parametrize("side", [1024, 2048, 4096])
 @pytest.mark.parametrize("radix,ctas", FOURSTEP_SHAPES)
-def test_fourstep_plan_matches_oracle(ctx, side, radix, ctas):
-    plan = {"impl": 3, "sched": 0, "l2_promo": 3, "blocked": 0, "stagger": 1, "radix": radix, "ctas": ctas}
-    cols = 1024 + 36  # ragged: not a whole number of tiles
-    data = O.seeded_input(side, cols, seed=side + radix + ctas)
+@pytest.mark.parametrize("blocked", [0, 1], ids=["three-launches", "pipelined"])
+def test_fourstep_plan_matches_oracle(ctx, side, radix, ctas, blocked):
+    plan = {"impl": 3, "sched": 0, "l2_promo": 3, "blocked": blocked, "stagger": 1, "radix": radix, "ctas": ctas}
+    cols = 1024 + 36  # ragged: not a whole number of tiles (the pipeline's last chunk is partial)
+    data = O.seeded_input(side, cols, seed=side + radix + ctas + blocked)
     ctx.plan_set(side, plan)
     try:
         d_out = torch.full((2 * side, cols), -1, dtype=torch.int32, device="cuda")
@@ -148,10 +149,34 @@ def test_fourstep_plan_matches_oracle(ctx, side, radix, ctas):
     assert np.array_equal(got, O.encode_rowmajor(data))
 
 
-def test_fourstep_plan_host_call(ctx):
+@pytest.mark.parametrize("side", [1024, 2048, 4096])
+@pytest.mark.parametrize("radix,ctas", FOURSTEP_SHAPES)
+def test_fourstep_pipeline_many_chunks(ctx, side, radix, ctas):
+    # the pipelined launch over hundreds of column chunks (many rounds of its work
+    # queue, chunks' passes overlapping) against the single-pass default plan, which
+    # the tests above pin to the oracle
+    cols = 65536 + 36
+    d_in = rand_dev(side, cols, seed=side + 7 * radix + ctas)
+    want = torch.empty((2 * side, cols), dtype=torch.int32, device="cuda")
+    ctx.extend(d_in, want, side, cols)
+    ctx.plan_set(side, {"impl": 3, "sched": 0, "l2_promo": 3, "blocked": 1, "stagger": 1, "radix": radix,
+                        "ctas": ctas})
+    try:
+        for _ in range(2):  # twice: the second launch starts from counters the first one left
+            got = torch.full((2 * side, cols), -1, dtype=torch.int32, device="cuda")
+            ctx.extend(d_in, got, side, cols)
+            torch.cuda.synchronize()
+            assert torch.equal(got, want)
+    finally:
+        ctx.plan_clear()
+
+
+@pytest.mark.parametrize("blocked", [0, 1], ids=["three-launches", "pipelined"])
+def test_fourstep_plan_host_call(ctx, blocked):
     # the host-buffer call runs the plan on odd rows only (the even rows are copied on the host)
     side, cols = 4096, 512
-    ctx.plan_set(side, {"impl": 3, "sched": 0, "l2_promo": 3, "blocked": 0, "stagger": 1, "radix": 8, "ctas": 2})
+    ctx.plan_set(side, {"impl": 3, "sched": 0, "l2_promo": 3, "blocked": blocked, "stagger": 1, "radix": 8,
+                        "ctas": 2})
     try:
         data = O.seeded_input(side, cols, seed=31)
         h_in = torch.from_numpy(data.view(np.int32)).pin_memory()

@@ -291,6 +291,8 @@ void zoda_ctx_destroy(zoda_ctx* c) {
             if (e) cudaEventDestroy(e);
     general_release(c);
     rlc_release(c);
+    c->pipe_cnt.release();
+    if (c->pipe_done) cudaEventDestroy(c->pipe_done);
     if (c->d_err) cudaFree(c->d_err);
     if (c->tables.tw) cudaFree(c->tables.tw);
     if (c->tables.tw_lo) cudaFree(c->tables.tw_lo);

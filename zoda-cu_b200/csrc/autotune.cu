@@ -92,13 +92,15 @@ std::vector<zoda_plan> candidates(int ls) {
                         add(p);
                     }
     }
-    if (ls >= FOURSTEP_MIN_LOG)  // three four-step passes, in each launch shape
+    // three four-step passes, in each launch shape: three launches over the square
+    // (blocked 0) or one launch that runs them column chunk by column chunk (1)
+    for (int blocked = 0; blocked <= 1 && ls >= FOURSTEP_MIN_LOG; blocked++)
         for (const auto& rc : {std::pair<int, int>{16, 1}, {16, 2}, {8, 2}, {8, 4}}) {
             zoda_plan p = d;
             p.impl = ZODA_IMPL_FOURSTEP;
             p.sched = 0;
             p.l2_promo = 3;
-            p.blocked = 0;
+            p.blocked = blocked;
             p.stagger = 1;
             p.radix = rc.first;
             p.ctas = rc.second;

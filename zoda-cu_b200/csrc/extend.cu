@@ -158,7 +158,7 @@ zoda_status launch_plan(const zoda_ctx* ctx, int log_s, const zoda_plan& p, cons
         // side's default plan instead
         if (in_rows == S && out_rows == 2 * S)
             return long_extend(ctx, log_s, ctx->tables.ext4[log_s], in, out, cols, st, odd_only,
-                               fourstep_shape(p.radix, p.ctas));
+                               fourstep_shape(p.radix, p.ctas), p.blocked != 0);
         return launch_plan(ctx, log_s, default_plan(log_s), in, out, cols, st, odd_only, in_rows, out_rows);
     }
     // stagger 1: release after all INTT levels but the last; 2: after the first; 3: right away

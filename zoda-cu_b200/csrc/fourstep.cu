@@ -106,6 +106,7 @@ StepArgs plain_args(View in, View out, uint32_t qpc, uint64_t nquads) {
     a.out = out;
     a.qpc = qpc;
     a.nquads = nquads;
+    a.qlim = ~0u;
     a.in_limit = NO_LIMIT;
     a.out_limit = NO_LIMIT;
     a.scale = Tw{1u, shoup(1u)};
@@ -179,6 +180,64 @@ zoda_status long_cols_ntt(const zoda_ctx* ctx, uint32_t* B, uint32_t* A, int L, 
     return run_step(ctx, L2, inv, pb, st);
 }
 
+// The same three passes in one persistent launch, column chunk by column chunk
+// (k_fourstep_pipe), so each chunk's intermediate stays in L2 between its passes.
+template <int L1, int L2, int SHAPE>
+zoda_status pipe_t(const zoda_ctx* ctx, const StepArgs pass[3], uint64_t cols, cudaStream_t st) {
+    using PS = PipeShape<L1, L2, SHAPE>;
+    using PA = typename PS::A::PL;
+    using PM = typename PS::M::PL;
+    const uint64_t quads = cols / 4;
+    const uint64_t nch = (quads + PS::CQ - 1) / PS::CQ;
+    PipeArgs pa{};
+    for (int i = 0; i < 3; i++) pa.pass[i] = pass[i];
+    const uint64_t NB2 = 1ull << L2, NB1 = 1ull << L1;  // column blocks of the strided / block passes
+    pa.pass[0].qpc = pa.pass[2].qpc = pa.pass[1].qpc = PS::CQ;
+    pa.pass[0].nquads = pa.pass[2].nquads = NB2 * PS::CQ;
+    pa.pass[1].nquads = NB1 * PS::CQ;
+    pa.tiles[0] = pa.tiles[2] = (uint32_t)(NB2 * PS::CQ / PA::Q4);
+    pa.tiles[1] = (uint32_t)(NB1 * PS::CQ / PM::Q4);
+    pa.chunk_u32 = 4ull * PS::CQ;
+    pa.nchunks = (uint32_t)nch;
+    pa.last_qlim = (uint32_t)(quads - (nch - 1) * PS::CQ);
+    const uint64_t grid = (uint64_t)ctx->sm_count * PS::MINB;
+    const uint64_t per_round = (uint64_t)pa.tiles[0] + pa.tiles[1] + pa.tiles[2];
+    // depth: enough rounds between a chunk's passes that its earlier tiles are done
+    // before the later ones are dealt (twice the items the CTAs hold at once)
+    uint64_t depth = (2 * 2 * grid + per_round - 1) / per_round;
+    if (depth < 1) depth = 1;
+    pa.depth = (uint32_t)depth;
+    if (nch > (1u << 30) || (nch + 2 * depth) * per_round + 2 * grid >= (1ull << 31)) return ZODA_ERR_UNSUPPORTED;
+    zoda_ctx* mc = const_cast<zoda_ctx*>(ctx);  // the pipeline's counters and ordering event
+    std::lock_guard<std::mutex> lock(mc->pipe_mu);
+    const size_t cbytes = (size_t)(1 + 2 * nch) * sizeof(uint32_t);
+    zoda_status s = mc->pipe_cnt.ensure(cbytes);
+    if (s != ZODA_OK) return s;
+    if (!mc->pipe_done) ZB_CUDA(cudaEventCreateWithFlags(&mc->pipe_done, cudaEventDisableTiming));
+    pa.counters = (uint32_t*)mc->pipe_cnt.p;
+    pa.err = ctx->d_err;
+    // launches on other streams share the counters: each waits for the one before
+    ZB_CUDA(cudaStreamWaitEvent(st, mc->pipe_done, 0));
+    ZB_CUDA(cudaMemsetAsync(pa.counters, 0, cbytes, st));
+    ZB_CUDA(cudaFuncSetAttribute(k_fourstep_pipe<L1, L2, SHAPE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)PS::SMEM));
+    k_fourstep_pipe<L1, L2, SHAPE><<<(unsigned)grid, PS::THREADS, PS::SMEM, st>>>(pa, ctx->tables.tw,
+                                                                                  ctx->tables.tw_lo);
+    ZB_CUDA(cudaGetLastError());
+    ZB_CUDA(cudaEventRecord(mc->pipe_done, st));
+    return ZODA_OK;
+}
+
+template <int L1, int L2>
+zoda_status pipe_shape(const zoda_ctx* ctx, int shape, const StepArgs pass[3], uint64_t cols, cudaStream_t st) {
+    switch (shape) {
+        case 1: return pipe_t<L1, L2, 1>(ctx, pass, cols, st);
+        case 2: return pipe_t<L1, L2, 2>(ctx, pass, cols, st);
+        case 3: return pipe_t<L1, L2, 3>(ctx, pass, cols, st);
+        default: return pipe_t<L1, L2, 0>(ctx, pass, cols, st);
+    }
+}
+
 // Extension of a square of side S = 2^L in three passes, 10 <= L <= 26 (above
 // 4096 no column fits one pass; from 1024 to 4096 it is an alternative plan): in
 // [S][cols] -> out [2S][cols]. The first pass writes the even rows (the input)
@@ -191,8 +250,9 @@ int fourstep_shape(int radix, int ctas) {
 }
 
 zoda_status long_extend(const zoda_ctx* ctx, int L, const uint2* tabs, const uint32_t* in, uint32_t* out,
-                        uint64_t cols, cudaStream_t st, bool odd_only, int shape) {
+                        uint64_t cols, cudaStream_t st, bool odd_only, int shape, bool pipelined) {
     if (L < FOURSTEP_MIN_LOG || L > LONG_MAX_LOG || cols % 4) return ZODA_ERR_UNSUPPORTED;
+    if (pipelined && L > PIPE_MAX_LOG) return ZODA_ERR_UNSUPPORTED;
     if (cols == 0) return ZODA_OK;
     const int L1 = L / 2, L2 = L - L1;
     const uint64_t N1 = 1ull << L1, N2 = 1ull << L2;
@@ -202,23 +262,37 @@ zoda_status long_extend(const zoda_ctx* ctx, int L, const uint2* tabs, const uin
     // odd rows: row r at odd + r * op (interleaved [2S][cols], or compact [S][cols] with odd_only)
     uint32_t* odd = odd_only ? out : out + cols;
     const uint64_t op = odd_only ? cols : 2 * cols;
+    StepArgs pass[3];
     // pass A (INTT over i1): input rows N2*i1 + i2 -> odd row N2*k1 + i2; the
     // loaded rows also go to the even rows
-    StepArgs pa = plain_args(View{const_cast<uint32_t*>(in), N2 * cols, cols}, View{odd, N2 * op, op}, qpc, N2 * qpc);
+    StepArgs& pa = pass[0];
+    pa = plain_args(View{const_cast<uint32_t*>(in), N2 * cols, cols}, View{odd, N2 * op, op}, qpc, N2 * qpc);
     pa.tw_log = L;
     pa.tw_inv = 1;
     if (!odd_only) pa.copy = View{out, 2 * N2 * cols, 2 * cols};
-    if ((s = run_step(ctx, L1, true, pa, st, shape)) != ZODA_OK) return s;
     // block pass, in place: INTT pass B over i2 in block k1, the twist g^i / S
     // (g = omega_2S), NTT pass A over the block's coefficients (decomposition
     // (N2, N1)), its twiddle omega_S^(k1 * m1)
-    StepArgs pm = plain_args(View{odd, op, N2 * op}, View{odd, op, N2 * op}, qpc, N1 * qpc);
+    StepArgs& pm = pass[1];
+    pm = plain_args(View{odd, op, N2 * op}, View{odd, op, N2 * op}, qpc, N1 * qpc);
     pm.mid1 = FTab{cbtab, 0, 1};
     pm.mid2 = FTab{ktab, 1, 0};
     pm.tw_log = L;
-    if ((s = run_step2(ctx, L2, true, pm, st, shape)) != ZODA_OK) return s;
     // pass B of the NTT, in place: wide rows j2 of column block m1 -> odd row m1 + N2*m2
-    StepArgs pb = plain_args(View{odd, N2 * op, op}, View{odd, N2 * op, op}, qpc, N2 * qpc);
+    StepArgs& pb = pass[2];
+    pb = plain_args(View{odd, N2 * op, op}, View{odd, N2 * op, op}, qpc, N2 * qpc);
+    if (pipelined) {
+        switch (L) {
+            case 10: return pipe_shape<5, 5>(ctx, shape, pass, cols, st);
+            case 11: return pipe_shape<5, 6>(ctx, shape, pass, cols, st);
+            case 12: return pipe_shape<6, 6>(ctx, shape, pass, cols, st);
+            case 13: return pipe_shape<6, 7>(ctx, shape, pass, cols, st);
+            case 14: return pipe_shape<7, 7>(ctx, shape, pass, cols, st);
+            default: return ZODA_ERR_UNSUPPORTED;
+        }
+    }
+    if ((s = run_step(ctx, L1, true, pa, st, shape)) != ZODA_OK) return s;
+    if ((s = run_step2(ctx, L2, true, pm, st, shape)) != ZODA_OK) return s;
     return run_step(ctx, L1, false, pb, st, shape);
 }
 

@@ -47,6 +47,7 @@ struct StepArgs {
     View copy;        // base != nullptr: every loaded input row is also stored here, unchanged
     uint32_t qpc;     // quads per column block
     uint64_t nquads;  // virtual quads of the pass
+    uint32_t qlim;    // quads at or past this index inside a column block are not real (a ragged chunk)
     // an input row whose index r * lim_rm + cb * lim_cm (its row in the
     // original matrix) is >= in_limit is zero and not read
     uint32_t in_lim_rm, in_lim_cm;
@@ -98,12 +99,32 @@ struct QuadPos {
         const uint32_t vv = active ? (uint32_t)v : 0u;
         cb = vv / a.qpc;
         qi = vv - cb * a.qpc;
+        active = active && qi < a.qlim;
     }
 };
 
+// Memory policies of a pass. Loads: streaming (evict-first, the default) or
+// through L2 only (LD_L2), for matrices another CTA of the same launch wrote, which
+// an SM's L1 may hold a stale copy of. Stores: streaming (the default) or kept
+// (ST_KEEP, the normal L2 policy) for intermediates the next pass reads soon.
+__device__ __forceinline__ V4 ldg_l2_v4(const uint32_t* p) {
+    uint4 u = __ldcg(reinterpret_cast<const uint4*>(p));
+    return V4{{u.x, u.y, u.z, u.w}};
+}
+template <bool LD_L2>
+__device__ __forceinline__ V4 step_ld(const uint32_t* p) {
+    if constexpr (LD_L2) return ldg_l2_v4(p);
+    return ldg_stream_v4(p);
+}
+template <bool ST_KEEP>
+__device__ __forceinline__ void step_st(uint32_t* p, const V4& v) {
+    if constexpr (ST_KEEP) st_v4(p, v);
+    else stg_stream_v4(p, v);
+}
+
 // Level 0 input: rows t + L0*j of the thread's quad, pre-factors applied, rows
 // past the limit (or with a zero factor) as zeros.
-template <class PL>
+template <class PL, bool LD_L2 = false>
 __device__ __forceinline__ void step_load(V4* v, const StepArgs& a, const QuadPos& p, int t) {
     constexpr int R0 = 1 << PL::lr(0);
     constexpr int L0 = PL::S / R0;
@@ -118,7 +139,7 @@ __device__ __forceinline__ void step_load(V4* v, const StepArgs& a, const QuadPo
             ld = f.w != 0;
         }
         if (ld) {
-            v[j] = ldg_stream_v4(src + (uint64_t)row * a.in.row_pitch);
+            v[j] = step_ld<LD_L2>(src + (uint64_t)row * a.in.row_pitch);
             if (a.copy.base)
                 stg_stream_v4(a.copy.base + (uint64_t)p.cb * a.copy.cb_pitch + 4ull * p.qi +
                                   (uint64_t)row * a.copy.row_pitch,
@@ -131,13 +152,15 @@ __device__ __forceinline__ void step_load(V4* v, const StepArgs& a, const QuadPo
 }
 
 // Output k of the thread's quad: post factors, then the store (if in range).
+template <bool ST_KEEP = false>
 __device__ __forceinline__ void step_store(V4 x, const StepArgs& a, const QuadPos& p, uint32_t k,
                                            const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo) {
     if (!p.active || (uint64_t)k * a.out_lim_rm + (uint64_t)p.cb * a.out_lim_cm >= a.out_limit) return;
     if (a.post.tab) mul4(x, ftab_at(a.post, k, p.cb));
     if (a.tw_log) mul_tw2d(x, p.cb * k, a.tw_log, a.tw_inv, tw, tw_lo);
     if (a.use_scale) mul4(x, a.scale);
-    stg_stream_v4(a.out.base + (uint64_t)p.cb * a.out.cb_pitch + 4ull * p.qi + (uint64_t)k * a.out.row_pitch, x);
+    step_st<ST_KEEP>(a.out.base + (uint64_t)p.cb * a.out.cb_pitch + 4ull * p.qi + (uint64_t)k * a.out.row_pitch,
+                     x);
 }
 
 // Launch shapes of the passes: level radix 2^LEPT, THREADS per CTA, MINB CTAs
@@ -156,38 +179,44 @@ struct StepShape {
     using PL = ExtPlan<LOG_N, 0, LEPT, THREADS>;
 };
 
+// One tile of a one-transform pass: N = 2^LOG_N points per virtual quad (INV:
+// inverse roots, unscaled) for the Q4 consecutive quads of tile `tile`.
+template <int LOG_N, bool INV, int SHAPE, bool LD_L2 = false, bool ST_KEEP = false>
+__device__ __forceinline__ void step_tile(const StepArgs& a, uint64_t tile, uint4* sm, int tid,
+                                          const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo) {
+    using PL = typename StepShape<LOG_N, SHAPE>::PL;
+    const int q = tid % PL::Q4;
+    const int t = tid / PL::Q4;
+    V4 v[PL::EPT];
+    const QuadPos p(tile * PL::Q4 + q, a);
+    step_load<PL, LD_L2>(v, a, p, t);
+    dif_levels<PL, 0, INV>(v, sm, t, q, tw);
+    using LV = Level<PL, PL::lr(PL::NLEV - 1), PL::pre(PL::NLEV - 1)>;
+#pragma unroll
+    for (int g = 0; g < LV::G; g++) {
+        const uint32_t blk = LV::gid(g, t);
+#pragma unroll
+        for (int r = 0; r < LV::R; r++) {
+            const uint32_t k =
+                digit_rev<PL, false>((blk << PL::lr(PL::NLEV - 1)) + (uint32_t)bitrev(r, PL::lr(PL::NLEV - 1)));
+            step_store<ST_KEEP>(v[g * LV::R + r], a, p, k, tw, tw_lo);
+        }
+    }
+}
+
 // One transform of N = 2^LOG_N points per virtual quad (INV: inverse roots,
 // unscaled), tiles of Q4 consecutive quads dealt round-robin.
 template <int LOG_N, bool INV, int SHAPE>
 __global__ void __launch_bounds__(StepShape<LOG_N, SHAPE>::THREADS, StepShape<LOG_N, SHAPE>::MINB)
     k_step(const StepArgs a, uint64_t ntiles, const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo) {
-    using PL = typename StepShape<LOG_N, SHAPE>::PL;
     extern __shared__ uint4 sm[];
-    const int tid = threadIdx.x;
-    const int q = tid % PL::Q4;
-    const int t = tid / PL::Q4;
-    V4 v[PL::EPT];
-    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const QuadPos p(tile * PL::Q4 + q, a);
-        step_load<PL>(v, a, p, t);
-        dif_levels<PL, 0, INV>(v, sm, t, q, tw);
-        using LV = Level<PL, PL::lr(PL::NLEV - 1), PL::pre(PL::NLEV - 1)>;
-#pragma unroll
-        for (int g = 0; g < LV::G; g++) {
-            const uint32_t blk = LV::gid(g, t);
-#pragma unroll
-            for (int r = 0; r < LV::R; r++) {
-                const uint32_t k = digit_rev<PL, false>((blk << PL::lr(PL::NLEV - 1)) +
-                                                        (uint32_t)bitrev(r, PL::lr(PL::NLEV - 1)));
-                step_store(v[g * LV::R + r], a, p, k, tw, tw_lo);
-            }
-        }
-    }
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+        step_tile<LOG_N, INV, SHAPE>(a, tile, sm, threadIdx.x, tw, tw_lo);
 }
 
 // The second transform's levels 1 .. NLEV-1 (mirrored radices, as ntt_levels in
 // extend.cuh, with either root direction); the last level stores every output.
-template <class PL, int l, bool INV2>
+template <class PL, int l, bool INV2, bool ST_KEEP = false>
 __device__ __forceinline__ void step2_levels(V4* v, uint4* sm, int t, int q, const Tw* tw, const Tw* tw_lo,
                                              const StepArgs& a, const QuadPos& p) {
     using LV = Level<PL, PL::nlr(l), PL::npre(l)>;
@@ -196,7 +225,7 @@ __device__ __forceinline__ void step2_levels(V4* v, uint4* sm, int t, int q, con
     if constexpr (l < PL::NLEV - 1) {
         LV::template twiddle_write<INV2>(v, sm, t, q, tw);
         __syncthreads();
-        step2_levels<PL, l + 1, INV2>(v, sm, t, q, tw, tw_lo, a, p);
+        step2_levels<PL, l + 1, INV2, ST_KEEP>(v, sm, t, q, tw, tw_lo, a, p);
     } else {
 #pragma unroll
         for (int g = 0; g < LV::G; g++) {
@@ -204,84 +233,229 @@ __device__ __forceinline__ void step2_levels(V4* v, uint4* sm, int t, int q, con
 #pragma unroll
             for (int r = 0; r < LV::R; r++) {
                 const uint32_t k = digit_rev<PL, true>((blk << PL::nlr(l)) + (uint32_t)bitrev(r, PL::nlr(l)));
-                step_store(v[g * LV::R + r], a, p, k, tw, tw_lo);
+                step_store<ST_KEEP>(v[g * LV::R + r], a, p, k, tw, tw_lo);
             }
         }
     }
 }
 
-// Two transforms of N = 2^LOG_N points per virtual quad with a factor between
-// them: out = T2( mid(k) * T1(pre * in)(k) ), T1 with roots w^-1 when INV1,
-// T2 with w^-1 when INV2, both unscaled. mid(k, cb) = mid1(k, cb) * mid2(k, cb).
-// With a counter, the nonzero outputs k >= count_from of T1 (before mid) are
-// counted (the decoder's consistency check).
+// One tile of a two-transform pass: out = T2( mid(k) * T1(pre * in)(k) ) over
+// N = 2^LOG_N points per virtual quad, T1 with roots w^-1 when INV1, T2 with w^-1
+// when INV2, both unscaled. mid(k, cb) = mid1(k, cb) * mid2(k, cb). With a
+// counter, the nonzero outputs k >= count_from of T1 (before mid) are added to
+// cnt (the decoder's consistency check).
+template <int LOG_N, bool INV1, bool INV2, int SHAPE, bool LD_L2 = false, bool ST_KEEP = false>
+__device__ __forceinline__ void step2_tile(const StepArgs& a, uint64_t tile, uint4* sm, int tid,
+                                           const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo,
+                                           unsigned long long& cnt) {
+    using PL = typename StepShape<LOG_N, SHAPE>::PL;
+    const int q = tid % PL::Q4;
+    const int t = tid / PL::Q4;
+    V4 v[PL::EPT];
+    const QuadPos p(tile * PL::Q4 + q, a);
+    step_load<PL, LD_L2>(v, a, p, t);
+    dif_levels<PL, 0, INV1>(v, sm, t, q, tw);
+    // T1's last level: group g (block b = g*TPQ + t) holds outputs c0 + (S/R)*j at
+    // v[g*R + bitrev(j)]; T2's first level (radix R over stride S/R) wants them in
+    // natural j order as its group n1 = c0, so no exchange sits between the two.
+    constexpr int LR = PL::lr(PL::NLEV - 1);
+    constexpr int R = 1 << LR;
+    constexpr int G = PL::EPT / R;
+    constexpr int SH = PL::LOG_S - LR;
+    uint32_t c0[G];
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+        const uint32_t b = (uint32_t)(g * PL::TPQ + t);
+        c0[g] = digit_rev<PL, false>(b << LR);
+        V4 y[R];
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            y[j] = v[g * R + bitrev(j, LR)];
+            const uint32_t k = c0[g] + ((uint32_t)j << SH);
+            if (a.counter && p.active && k >= a.count_from)
+#pragma unroll
+                for (int e = 0; e < 4; e++) cnt += y[j].c[e] != 0;
+            if (a.mid1.tab) mul4(y[j], ftab_at(a.mid1, k, p.cb));
+            if (a.mid2.tab) mul4(y[j], ftab_at(a.mid2, k, p.cb));
+        }
+#pragma unroll
+        for (int j = 0; j < R; j++) v[g * R + j] = y[j];
+    }
+    // T2 level 0: radix R over stride S/R, one block; group n1 = c0
+#pragma unroll
+    for (int g = 0; g < G; g++) dft_dif<LR, INV2>(v + g * R);
+    if constexpr (PL::NLEV > 1) {
+        __syncthreads();  // every thread finished reading T1's last level
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const int k2 = bitrev(r, LR);
+                V4 x = v[g * R + r];
+                if (k2 != 0) mul4(x, tw_at<INV2>(tw, c0[g] * (uint32_t)k2, PL::LOG_S));
+                sm[(size_t)(c0[g] + ((uint32_t)k2 << SH)) * PL::Q4 + q] =
+                    make_uint4(x.c[0], x.c[1], x.c[2], x.c[3]);
+            }
+        }
+        __syncthreads();
+        step2_levels<PL, 1, INV2, ST_KEEP>(v, sm, t, q, tw, tw_lo, a, p);
+    } else {
+#pragma unroll
+        for (int r = 0; r < R; r++) step_store<ST_KEEP>(v[r], a, p, (uint32_t)bitrev(r, LR), tw, tw_lo);
+    }
+}
+
+// Two transforms per virtual quad with a factor between them (step2_tile), tiles
+// of Q4 consecutive quads dealt round-robin.
 template <int LOG_N, bool INV1, bool INV2, int SHAPE>
 __global__ void __launch_bounds__(StepShape<LOG_N, SHAPE>::THREADS, StepShape<LOG_N, SHAPE>::MINB)
     k_step2(const StepArgs a, uint64_t ntiles, const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo) {
-    using PL = typename StepShape<LOG_N, SHAPE>::PL;
     extern __shared__ uint4 sm[];
     const int tid = threadIdx.x;
-    const int q = tid % PL::Q4;
-    const int t = tid / PL::Q4;
     unsigned long long cnt = 0;
-    V4 v[PL::EPT];
-    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const QuadPos p(tile * PL::Q4 + q, a);
-        step_load<PL>(v, a, p, t);
-        dif_levels<PL, 0, INV1>(v, sm, t, q, tw);
-        // T1's last level: group g (block b = g*TPQ + t) holds outputs c0 + (S/R)*j at
-        // v[g*R + bitrev(j)]; T2's first level (radix R over stride S/R) wants them in
-        // natural j order as its group n1 = c0, so no exchange sits between the two.
-        constexpr int LR = PL::lr(PL::NLEV - 1);
-        constexpr int R = 1 << LR;
-        constexpr int G = PL::EPT / R;
-        constexpr int SH = PL::LOG_S - LR;
-        uint32_t c0[G];
-#pragma unroll
-        for (int g = 0; g < G; g++) {
-            const uint32_t b = (uint32_t)(g * PL::TPQ + t);
-            c0[g] = digit_rev<PL, false>(b << LR);
-            V4 y[R];
-#pragma unroll
-            for (int j = 0; j < R; j++) {
-                y[j] = v[g * R + bitrev(j, LR)];
-                const uint32_t k = c0[g] + ((uint32_t)j << SH);
-                if (a.counter && p.active && k >= a.count_from)
-#pragma unroll
-                    for (int e = 0; e < 4; e++) cnt += y[j].c[e] != 0;
-                if (a.mid1.tab) mul4(y[j], ftab_at(a.mid1, k, p.cb));
-                if (a.mid2.tab) mul4(y[j], ftab_at(a.mid2, k, p.cb));
-            }
-#pragma unroll
-            for (int j = 0; j < R; j++) v[g * R + j] = y[j];
-        }
-        // T2 level 0: radix R over stride S/R, one block; group n1 = c0
-#pragma unroll
-        for (int g = 0; g < G; g++) dft_dif<LR, INV2>(v + g * R);
-        if constexpr (PL::NLEV > 1) {
-            __syncthreads();  // every thread finished reading T1's last level
-#pragma unroll
-            for (int g = 0; g < G; g++) {
-#pragma unroll
-                for (int r = 0; r < R; r++) {
-                    const int k2 = bitrev(r, LR);
-                    V4 x = v[g * R + r];
-                    if (k2 != 0) mul4(x, tw_at<INV2>(tw, c0[g] * (uint32_t)k2, PL::LOG_S));
-                    sm[(size_t)(c0[g] + ((uint32_t)k2 << SH)) * PL::Q4 + q] =
-                        make_uint4(x.c[0], x.c[1], x.c[2], x.c[3]);
-                }
-            }
-            __syncthreads();
-            step2_levels<PL, 1, INV2>(v, sm, t, q, tw, tw_lo, a, p);
-        } else {
-#pragma unroll
-            for (int r = 0; r < R; r++) step_store(v[r], a, p, (uint32_t)bitrev(r, LR), tw, tw_lo);
-        }
-    }
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+        step2_tile<LOG_N, INV1, INV2, SHAPE>(a, tile, sm, tid, tw, tw_lo, cnt);
     if (a.counter) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xFFFFFFFFu, cnt, o);
         if ((tid & 31) == 0 && cnt) atomicAdd(a.counter, cnt);
+    }
+}
+
+// ---- the extension's three passes in one persistent launch, chunk by chunk ----
+// The three passes of a square's extension (strided INTT pass A, block pass,
+// strided NTT pass B) each read and write a whole matrix. Run one after the
+// other over the square, every intermediate goes to HBM and back: 56 bytes per
+// input element at side 4096 against the 12 the extension must move. Here the
+// columns are cut into chunks of CQ quads, and one persistent launch runs the
+// passes chunk by chunk, a few chunks apart, so a chunk's intermediate (its odd
+// output rows) is still in L2 when the next pass reads it.
+//
+// Work items are the tiles of (chunk, pass). Round r holds, in this order, the
+// tiles of pass A of chunk r, of the block pass of chunk r - depth and of pass B
+// of chunk r - 2*depth (chunks out of range are empty items); a global counter
+// deals items in that order. The block pass of a chunk waits until all its pass-A
+// tiles are done (a per-chunk counter), pass B until all its block tiles are. An
+// item waits only on items dealt before it, to CTAs that are running them, so
+// the launch cannot deadlock whatever the number of resident CTAs. Each wait is
+// bounded; on expiry the CTA flags the error (bit 4) and leaves.
+//
+// Matrices a pass reads after another CTA of the launch wrote them are loaded
+// through L2 only (an SM's L1 may hold a stale copy of a line); intermediates
+// are stored with the normal L2 policy, streamed data (the input, the even rows,
+// the final odd rows) with evict-first.
+struct PipeArgs {
+    StepArgs pass[3];    // chunk 0's views; qpc = CQ, nquads = blocks * CQ
+    uint64_t chunk_u32;  // u32 from one chunk's first column to the next chunk's
+    uint32_t nchunks;
+    uint32_t last_qlim;  // real quads in the last chunk
+    uint32_t tiles[3];   // tiles per chunk of each pass
+    uint32_t depth;      // rounds between a chunk's passes
+    uint32_t* counters;  // [0] item counter; [1 + c] pass-A tiles done; [1 + nchunks + c] block tiles done
+    int* err;
+};
+
+constexpr uint32_t PIPE_WAIT_POLLS = 1u << 21;  // about a second of polling
+
+__device__ __forceinline__ bool pipe_wait_count(const uint32_t* p, uint32_t need) {
+    for (uint32_t i = 0; i < PIPE_WAIT_POLLS; i++) {
+        uint32_t v;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+        if (v >= need) return true;
+        __nanosleep(64);
+    }
+    return false;
+}
+
+template <int PH, int L1, int L2, int SHAPE>
+__device__ __forceinline__ void pipe_pass(const PipeArgs& pa, uint32_t c, uint32_t tile, uint4* sm, int tid,
+                                          const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo) {
+    StepArgs x = pa.pass[PH];
+    const uint64_t off = (uint64_t)c * pa.chunk_u32;
+    x.in.base += off;
+    x.out.base += off;
+    if (x.copy.base) x.copy.base += off;
+    if (c + 1 == pa.nchunks) x.qlim = pa.last_qlim;
+    if constexpr (PH == 0) {
+        step_tile<L1, true, SHAPE, false, true>(x, tile, sm, tid, tw, tw_lo);
+    } else if constexpr (PH == 1) {
+        unsigned long long cnt = 0;
+        step2_tile<L2, true, false, SHAPE, true, true>(x, tile, sm, tid, tw, tw_lo, cnt);
+    } else {
+        step_tile<L1, false, SHAPE, true, false>(x, tile, sm, tid, tw, tw_lo);
+    }
+}
+
+template <int L1, int L2, int SHAPE>
+struct PipeShape {
+    using A = StepShape<L1, SHAPE>;
+    using M = StepShape<L2, SHAPE>;
+    static_assert(A::THREADS == M::THREADS && A::MINB == M::MINB, "one CTA shape for all passes");
+    static constexpr int THREADS = A::THREADS, MINB = A::MINB;
+    static constexpr size_t SMEM = A::PL::SMEM > M::PL::SMEM ? A::PL::SMEM : M::PL::SMEM;
+    static constexpr uint32_t CQ = A::PL::Q4 > M::PL::Q4 ? A::PL::Q4 : M::PL::Q4;  // quads per chunk
+};
+
+template <int L1, int L2, int SHAPE>
+__global__ void __launch_bounds__(PipeShape<L1, L2, SHAPE>::THREADS, PipeShape<L1, L2, SHAPE>::MINB)
+    k_fourstep_pipe(const __grid_constant__ PipeArgs pa, const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo) {
+    extern __shared__ uint4 sm[];
+    __shared__ uint32_t s_item;
+    __shared__ int s_fail;
+    const int tid = threadIdx.x;
+    const uint32_t per_round = pa.tiles[0] + pa.tiles[1] + pa.tiles[2];
+    const uint32_t total = (pa.nchunks + 2 * pa.depth) * per_round;  // the host keeps this below 2^31
+    if (tid == 0) {
+        s_item = atomicAdd(pa.counters, 1u);
+        s_fail = 0;
+    }
+    __syncthreads();
+    uint32_t item = s_item;
+    while (item < total) {
+        __syncthreads();  // every thread has read s_item
+        uint32_t nxt = 0;
+        if (tid == 0) nxt = atomicAdd(pa.counters, 1u);  // drawn now, used after the tile
+        const uint32_t r = item / per_round;
+        uint32_t j = item - r * per_round;
+        int ph = 0;
+        int64_t c = r;
+        if (j >= pa.tiles[0]) {
+            j -= pa.tiles[0];
+            if (j < pa.tiles[1]) {
+                ph = 1;
+                c = (int64_t)r - pa.depth;
+            } else {
+                j -= pa.tiles[1];
+                ph = 2;
+                c = (int64_t)r - 2 * (int64_t)pa.depth;
+            }
+        }
+        if (c >= 0 && c < (int64_t)pa.nchunks) {
+            const uint32_t cc = (uint32_t)c;
+            if (ph > 0) {
+                if (tid == 0) {
+                    const uint32_t* done = pa.counters + 1 + (ph == 1 ? 0u : pa.nchunks) + cc;
+                    if (!pipe_wait_count(done, pa.tiles[ph - 1])) {
+                        s_fail = 1;
+                        atomicOr(pa.err, 4);
+                    }
+                    __threadfence();
+                }
+                __syncthreads();
+                if (s_fail) return;
+            }
+            if (ph == 0) pipe_pass<0, L1, L2, SHAPE>(pa, cc, j, sm, tid, tw, tw_lo);
+            else if (ph == 1) pipe_pass<1, L1, L2, SHAPE>(pa, cc, j, sm, tid, tw, tw_lo);
+            else pipe_pass<2, L1, L2, SHAPE>(pa, cc, j, sm, tid, tw, tw_lo);
+            if (ph < 2) {
+                __threadfence();  // this thread's stores of the tile, before the count
+                __syncthreads();
+                if (tid == 0) atomicAdd(pa.counters + 1 + (ph == 0 ? 0u : pa.nchunks) + cc, 1u);
+            }
+        }
+        if (tid == 0) s_item = nxt;
+        __syncthreads();
+        item = s_item;
     }
 }
 

@@ -105,6 +105,11 @@ struct zoda_ctx {
     zb::DevBuf gen_a, gen_b, gen_tab, gen_small;
     std::map<int, zb::DevBuf> coset_tabs;
     cudaEvent_t gen_done = nullptr;
+    // the pipelined four-step launch (fourstep.cu): per-chunk counters, their lock,
+    // and an event after the last launch that used them
+    zb::DevBuf pipe_cnt;
+    std::mutex pipe_mu;
+    cudaEvent_t pipe_done = nullptr;
     // RLC consumers (rlc.cu): canonical coefficient table, row
     // accumulators and the check's matrices, under their own lock
     zb::DevBuf rlc_w, rlc_acc, rlc_d, rlc_e, rlc_f, rlc_cnt;
@@ -152,12 +157,16 @@ zoda_status long_cols_ntt(const zoda_ctx* ctx, uint32_t* B, uint32_t* A, int L, 
 // The coset factor tables of the long encode over 2^ln points with n_k = 2^L (built
 // once, kept in ctx->coset_tabs: call it holding ctx->mu).
 zoda_status coset_mid_tables(zoda_ctx* ctx, int L, int ln, const uint2** tabs);
-// Extension of a 2^L square (12 <= L <= 26) in three passes, the odd output rows as
+// Extension of a 2^L square (10 <= L <= 26) in three passes, the odd output rows as
 // scratch; odd_only: out is the compact [S][cols] odd rows (the even rows are the input).
 // tabs = coset_mid_tables(ctx, L, L + 1).
-// shape: the launch shape of the passes (fourstep.cuh, StepShape).
+// shape: the launch shape of the passes (fourstep.cuh, StepShape). pipelined (L <=
+// PIPE_MAX_LOG): one persistent launch runs the passes column chunk by column chunk
+// (k_fourstep_pipe) instead of three launches over the whole square.
+constexpr int PIPE_MAX_LOG = 14;
 zoda_status long_extend(const zoda_ctx* ctx, int L, const uint2* tabs, const uint32_t* in, uint32_t* out,
-                        uint64_t cols, cudaStream_t st, bool odd_only = false, int shape = 0);
+                        uint64_t cols, cudaStream_t st, bool odd_only = false, int shape = 0,
+                        bool pipelined = false);
 // The four-step launch shape of a plan's (radix, ctas).
 int fourstep_shape(int radix, int ctas);
 // Smallest side (log2) the four-step plan covers.
