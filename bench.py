@@ -306,18 +306,23 @@ def time_long_leg(ctx) -> dict:
         res["same_result"] = bool(np.array_equal(a, b))
     sq.free()
     out["cuda_ntt_131072"] = res
-    side, cols = 4096, 4096 * SHARE_U32
-    shapes = {}
-    for blocked in (0, 1):  # three launches over the square, or one pipelined launch chunk by chunk
-        for radix, ctas in ((16, 1), (16, 2), (8, 2), (8, 4)):
-            ctx.plan_set(side, {"impl": 3, "sched": 0, "l2_promo": 3, "blocked": blocked, "stagger": 1,
-                                "radix": radix, "ctas": ctas})
-            ms, _, check = time_device_extend(ctx, side, 5, 2, 1, verify=(radix, ctas) == (8, 2), cols=cols)
-            shapes[f"{'pipelined' if blocked else 'three_launches'}_radix{radix}_ctas{ctas}"] = {
-                "ms": round(ms / 5, 4), "check_mismatches": check["check_mismatches"] if check else None}
-            torch.cuda.empty_cache()
-    ctx.plan_clear()
-    out["fourstep_side4096"] = shapes
+    for side in (1024, 2048, 4096):
+        cols = side * SHARE_U32
+        shapes = {}
+        # three launches over the square, the same with cp.async-staged tiles, or one
+        # pipelined launch chunk by chunk
+        for form, (sched, blocked) in (("three_launches", (0, 0)), ("staged", (1, 0)), ("pipelined", (0, 1))):
+            for radix, ctas in ((16, 1), (16, 2), (8, 2), (8, 4)):
+                if form == "staged" and ctas == 1:
+                    continue
+                ctx.plan_set(side, {"impl": 3, "sched": sched, "l2_promo": 3, "blocked": blocked, "stagger": 1,
+                                    "radix": radix, "ctas": ctas})
+                ms, _, check = time_device_extend(ctx, side, 5, 2, 1, verify=(radix, ctas) == (8, 2), cols=cols)
+                shapes[f"{form}_radix{radix}_ctas{ctas}"] = {
+                    "ms": round(ms / 5, 4), "check_mismatches": check["check_mismatches"] if check else None}
+                torch.cuda.empty_cache()
+        ctx.plan_clear()
+        out[f"fourstep_side{side}"] = shapes
     return out
 
 
@@ -876,12 +881,19 @@ def main():
     ap.add_argument("--cols", type=int, default=0, help="columns of the extend leg (0: side * 128)")
     ap.add_argument("--force-impl", choices=["auto", "direct", "tma"], default="auto",
                     help="legs only: run one kernel family with default knobs instead of the side's plan")
+    ap.add_argument("--plan", default=None,
+                    help="legs only: a JSON launch plan installed for --side (zoda_plan fields), e.g. "
+                         "'{\"impl\": 3, \"radix\": 8, \"ctas\": 4, \"blocked\": 1}'")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps
     if args.leg:
         import zoda_b200
         ctx = zoda_b200.Context(0)
         ctx.set_impl({"auto": 0, "direct": 1, "tma": 2}[args.force_impl])
+        if args.plan:
+            plan = {"impl": 1, "sched": 0, "l2_promo": 3, "blocked": 0, "stagger": 1, "radix": 16, "ctas": 0}
+            plan.update(json.loads(args.plan))
+            ctx.plan_set(args.side, plan)
         leg = {"rlc": lambda: time_rlc(ctx, 1024), "recover": lambda: time_recover(ctx, 1024),
                "encode": lambda: [time_encode_general(ctx, 1000, 1000), time_encode_general(ctx, 1000, 3000)],
                "extend": lambda: time_extend_leg(ctx, args.side, args.cols or args.side * SHARE_U32, args.steps,

@@ -131,13 +131,20 @@ def test_long_extension_matches_oracle(ctx, side, cols):
 FOURSTEP_SHAPES = [(16, 1), (16, 2), (8, 2), (8, 4)]
 
 
+# plan forms: (sched, blocked) = three launches, three staged launches (cp.async
+# prefetch of each next tile), one pipelined launch
+FORMS = {"three-launches": (0, 0), "staged": (1, 0), "pipelined": (0, 1)}
+FOURSTEP_PLANS = [(f, r, c) for f in FORMS for r, c in FOURSTEP_SHAPES if not (f == "staged" and c == 1)]
+
+
 @pytest.mark.parametrize("side", [1024, 2048, 4096])
-@pytest.mark.parametrize("radix,ctas", FOURSTEP_SHAPES)
-@pytest.mark.parametrize("blocked", [0, 1], ids=["three-launches", "pipelined"])
-def test_fourstep_plan_matches_oracle(ctx, side, radix, ctas, blocked):
-    plan = {"impl": 3, "sched": 0, "l2_promo": 3, "blocked": blocked, "stagger": 1, "radix": radix, "ctas": ctas}
+@pytest.mark.parametrize("form,radix,ctas", FOURSTEP_PLANS)
+def test_fourstep_plan_matches_oracle(ctx, side, form, radix, ctas):
+    sched, blocked = FORMS[form]
+    plan = {"impl": 3, "sched": sched, "l2_promo": 3, "blocked": blocked, "stagger": 1, "radix": radix,
+            "ctas": ctas}
     cols = 1024 + 36  # ragged: not a whole number of tiles (the pipeline's last chunk is partial)
-    data = O.seeded_input(side, cols, seed=side + radix + ctas + blocked)
+    data = O.seeded_input(side, cols, seed=side + radix + ctas + 3 * sched + blocked)
     ctx.plan_set(side, plan)
     try:
         d_out = torch.full((2 * side, cols), -1, dtype=torch.int32, device="cuda")
@@ -150,16 +157,17 @@ def test_fourstep_plan_matches_oracle(ctx, side, radix, ctas, blocked):
 
 
 @pytest.mark.parametrize("side", [1024, 2048, 4096])
-@pytest.mark.parametrize("radix,ctas", FOURSTEP_SHAPES)
-def test_fourstep_pipeline_many_chunks(ctx, side, radix, ctas):
+@pytest.mark.parametrize("form,radix,ctas", [p for p in FOURSTEP_PLANS if p[0] != "three-launches"])
+def test_fourstep_many_tiles(ctx, side, form, radix, ctas):
     # the pipelined launch over hundreds of column chunks (many rounds of its work
-    # queue, chunks' passes overlapping) against the single-pass default plan, which
-    # the tests above pin to the oracle
+    # queue, chunks' passes overlapping), and the staged passes over many tiles per
+    # CTA, against the single-pass default plan, which the tests above pin to the oracle
+    sched, blocked = FORMS[form]
     cols = 65536 + 36
     d_in = rand_dev(side, cols, seed=side + 7 * radix + ctas)
     want = torch.empty((2 * side, cols), dtype=torch.int32, device="cuda")
     ctx.extend(d_in, want, side, cols)
-    ctx.plan_set(side, {"impl": 3, "sched": 0, "l2_promo": 3, "blocked": 1, "stagger": 1, "radix": radix,
+    ctx.plan_set(side, {"impl": 3, "sched": sched, "l2_promo": 3, "blocked": blocked, "stagger": 1, "radix": radix,
                         "ctas": ctas})
     try:
         for _ in range(2):  # twice: the second launch starts from counters the first one left
@@ -171,11 +179,12 @@ def test_fourstep_pipeline_many_chunks(ctx, side, radix, ctas):
         ctx.plan_clear()
 
 
-@pytest.mark.parametrize("blocked", [0, 1], ids=["three-launches", "pipelined"])
-def test_fourstep_plan_host_call(ctx, blocked):
+@pytest.mark.parametrize("form", list(FORMS))
+def test_fourstep_plan_host_call(ctx, form):
     # the host-buffer call runs the plan on odd rows only (the even rows are copied on the host)
     side, cols = 4096, 512
-    ctx.plan_set(side, {"impl": 3, "sched": 0, "l2_promo": 3, "blocked": blocked, "stagger": 1, "radix": 8,
+    sched, blocked = FORMS[form]
+    ctx.plan_set(side, {"impl": 3, "sched": sched, "l2_promo": 3, "blocked": blocked, "stagger": 1, "radix": 8,
                         "ctas": 2})
     try:
         data = O.seeded_input(side, cols, seed=31)

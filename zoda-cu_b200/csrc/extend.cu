@@ -130,6 +130,9 @@ zoda_status check_plan(int log_s, const zoda_plan& p) {
         if (p.ctas < 0 || p.ctas > 4 || p.ctas == 3 || (p.radix == 16 && p.ctas == 4) ||
             (p.radix == 8 && p.ctas <= 1))
             return ZODA_ERR_ARG;
+        // sched 1: staged passes, which exist for the shapes of 2 and 4 CTAs per SM
+        // and the three-launch form
+        if (p.sched == 1 && (p.ctas <= 1 || p.blocked)) return ZODA_ERR_ARG;
     }
     if (p.sched < 0 || p.sched > 1 || p.l2_promo < 0 || p.l2_promo > 3 || p.blocked < 0 || p.blocked > 1 ||
         p.stagger < 0 || p.stagger > 3 || (p.radix != 16 && p.radix != 8))
@@ -158,7 +161,7 @@ zoda_status launch_plan(const zoda_ctx* ctx, int log_s, const zoda_plan& p, cons
         // side's default plan instead
         if (in_rows == S && out_rows == 2 * S)
             return long_extend(ctx, log_s, ctx->tables.ext4[log_s], in, out, cols, st, odd_only,
-                               fourstep_shape(p.radix, p.ctas), p.blocked != 0);
+                               fourstep_shape(p.radix, p.ctas, p.sched != 0), p.blocked != 0);
         return launch_plan(ctx, log_s, default_plan(log_s), in, out, cols, st, odd_only, in_rows, out_rows);
     }
     // stagger 1: release after all INTT levels but the last; 2: after the first; 3: right away

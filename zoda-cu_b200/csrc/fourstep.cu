@@ -23,78 +23,115 @@
 namespace zb {
 namespace {
 
-template <int LOG_N, bool INV, int SHAPE>
+// Grid of a pass: one round of tiles over the resident CTAs, at most.
+inline unsigned pass_grid(const zoda_ctx* ctx, uint64_t ntiles, int minb) {
+    const uint64_t cap = (uint64_t)ctx->sm_count * minb;
+    return (unsigned)(ntiles < cap ? ntiles : cap);
+}
+
+// One pass of any features (F = SF_ALL), or of a feature set the caller fixes.
+template <int LOG_N, bool INV, int SHAPE, int F = SF_ALL>
 zoda_status step_t(const zoda_ctx* ctx, const StepArgs& a, cudaStream_t st) {
     using SH = StepShape<LOG_N, SHAPE>;
     using PL = typename SH::PL;
     const uint64_t ntiles = (a.nquads + PL::Q4 - 1) / PL::Q4;
     if (ntiles == 0) return ZODA_OK;
     if (PL::SMEM > 0)
-        ZB_CUDA(cudaFuncSetAttribute(k_step<LOG_N, INV, SHAPE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        ZB_CUDA(cudaFuncSetAttribute(k_step<LOG_N, INV, SHAPE, F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)PL::SMEM));
-    const uint64_t cap = (uint64_t)ctx->sm_count * SH::MINB;
-    const uint64_t grid = ntiles < cap ? ntiles : cap;
-    k_step<LOG_N, INV, SHAPE><<<(unsigned)grid, PL::THREADS, PL::SMEM, st>>>(a, ntiles, ctx->tables.tw,
-                                                                            ctx->tables.tw_lo);
+    k_step<LOG_N, INV, SHAPE, F><<<pass_grid(ctx, ntiles, SH::MINB), PL::THREADS, PL::SMEM, st>>>(
+        a, ntiles, ctx->tables.tw, ctx->tables.tw_lo);
     ZB_CUDA(cudaGetLastError());
     return ZODA_OK;
 }
 
-template <int LOG_N, bool INV1, int SHAPE>
+template <int LOG_N, bool INV1, int SHAPE, int F = SF_ALL>
 zoda_status step2_t(const zoda_ctx* ctx, const StepArgs& a, cudaStream_t st) {
     using SH = StepShape<LOG_N, SHAPE>;
     using PL = typename SH::PL;
     const uint64_t ntiles = (a.nquads + PL::Q4 - 1) / PL::Q4;
     if (ntiles == 0) return ZODA_OK;
     if (PL::SMEM > 0)
-        ZB_CUDA(cudaFuncSetAttribute(k_step2<LOG_N, INV1, !INV1, SHAPE>,
+        ZB_CUDA(cudaFuncSetAttribute(k_step2<LOG_N, INV1, !INV1, SHAPE, F>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PL::SMEM));
-    const uint64_t cap = (uint64_t)ctx->sm_count * SH::MINB;
-    const uint64_t grid = ntiles < cap ? ntiles : cap;
-    k_step2<LOG_N, INV1, !INV1, SHAPE><<<(unsigned)grid, PL::THREADS, PL::SMEM, st>>>(a, ntiles, ctx->tables.tw,
-                                                                                     ctx->tables.tw_lo);
+    k_step2<LOG_N, INV1, !INV1, SHAPE, F><<<pass_grid(ctx, ntiles, SH::MINB), PL::THREADS, PL::SMEM, st>>>(
+        a, ntiles, ctx->tables.tw, ctx->tables.tw_lo);
     ZB_CUDA(cudaGetLastError());
     return ZODA_OK;
 }
 
-template <int LOG_N, int SHAPE>
-zoda_status step_any(const zoda_ctx* ctx, bool two, bool inv, const StepArgs& a, cudaStream_t st) {
-    if (two) return inv ? step2_t<LOG_N, true, SHAPE>(ctx, a, st) : step2_t<LOG_N, false, SHAPE>(ctx, a, st);
-    return inv ? step_t<LOG_N, true, SHAPE>(ctx, a, st) : step_t<LOG_N, false, SHAPE>(ctx, a, st);
-}
-
-template <int LOG_N>
-zoda_status step_shape(const zoda_ctx* ctx, int shape, bool two, bool inv, const StepArgs& a, cudaStream_t st) {
-    if constexpr (LOG_N <= STEP_SHAPE_MAX_LOG) {
-        switch (shape) {
-            case 1: return step_any<LOG_N, 1>(ctx, two, inv, a, st);
-            case 2: return step_any<LOG_N, 2>(ctx, two, inv, a, st);
-            case 3: return step_any<LOG_N, 3>(ctx, two, inv, a, st);
-            default: break;
-        }
-    }
-    return step_any<LOG_N, 0>(ctx, two, inv, a, st);
+// The staged pass (k_step_st): two tiles of shared memory, the next one arriving
+// by cp.async while the current one computes.
+template <int LOG_N, bool INV, bool TWO, int SHAPE, int F>
+zoda_status step_st_t(const zoda_ctx* ctx, const StepArgs& a, cudaStream_t st) {
+    using SH = StepShape<LOG_N, SHAPE>;
+    using PL = typename SH::PL;
+    static_assert(SH::MINB_ST >= 1, "two tiles fit one SM");
+    const uint64_t ntiles = (a.nquads + PL::Q4 - 1) / PL::Q4;
+    if (ntiles == 0) return ZODA_OK;
+    constexpr size_t smem = 2 * PL::SMEM;
+    ZB_CUDA(cudaFuncSetAttribute(k_step_st<LOG_N, INV, TWO, SHAPE, F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+    k_step_st<LOG_N, INV, TWO, SHAPE, F><<<pass_grid(ctx, ntiles, SH::MINB_ST), PL::THREADS, smem, st>>>(
+        a, ntiles, ctx->tables.tw, ctx->tables.tw_lo);
+    ZB_CUDA(cudaGetLastError());
+    return ZODA_OK;
 }
 
 // One transform (two = false) or two fused transforms (two: INTT then NTT when
 // inv, else NTT then INTT) of 2^log_n points (5 <= log_n <= 13) per virtual
-// quad, in launch shape `shape` (shapes 1..3 apply up to 256 points).
-zoda_status run_pass(const zoda_ctx* ctx, int log_n, bool two, bool inv, const StepArgs& a, cudaStream_t st,
-                     int shape = 0) {
+// quad, every feature available, one CTA per SM.
+zoda_status run_pass(const zoda_ctx* ctx, int log_n, bool two, bool inv, const StepArgs& a, cudaStream_t st) {
     switch (log_n) {
-#define ZB_CASE(L) \
-    case L: return step_shape<L>(ctx, shape, two, inv, a, st);
+#define ZB_CASE(L)                                                                                     \
+    case L:                                                                                            \
+        if (two) return inv ? step2_t<L, true, 0>(ctx, a, st) : step2_t<L, false, 0>(ctx, a, st);     \
+        return inv ? step_t<L, true, 0>(ctx, a, st) : step_t<L, false, 0>(ctx, a, st);
         ZB_CASE(5) ZB_CASE(6) ZB_CASE(7) ZB_CASE(8) ZB_CASE(9) ZB_CASE(10) ZB_CASE(11) ZB_CASE(12) ZB_CASE(13)
 #undef ZB_CASE
         default: return ZODA_ERR_UNSUPPORTED;
     }
 }
-zoda_status run_step(const zoda_ctx* ctx, int log_n, bool inv, const StepArgs& a, cudaStream_t st, int shape = 0) {
-    return run_pass(ctx, log_n, false, inv, a, st, shape);
+zoda_status run_step(const zoda_ctx* ctx, int log_n, bool inv, const StepArgs& a, cudaStream_t st) {
+    return run_pass(ctx, log_n, false, inv, a, st);
 }
-zoda_status run_step2(const zoda_ctx* ctx, int log_n, bool inv1, const StepArgs& a, cudaStream_t st,
-                      int shape = 0) {
-    return run_pass(ctx, log_n, true, inv1, a, st, shape);
+zoda_status run_step2(const zoda_ctx* ctx, int log_n, bool inv1, const StepArgs& a, cudaStream_t st) {
+    return run_pass(ctx, log_n, true, inv1, a, st);
+}
+
+// The passes of a square's extension (long_extend, sides up to 2^PIPE_MAX_LOG), with
+// only the features each one uses: PASS 0 = the strided INTT pass (twiddle, even-row
+// copy), 1 = the block pass (middle factors, twiddle), 2 = the strided NTT pass.
+// shape: 0..3 (fourstep.cuh StepShape), plus STEP_STAGED for the staged form.
+template <int LOG_N, int PASS, int SHAPE>
+zoda_status ext_pass_t(const zoda_ctx* ctx, bool staged, const StepArgs& a, cudaStream_t st) {
+    constexpr int F = PASS == 0 ? SF_EXT_A : PASS == 1 ? SF_EXT_M : SF_EXT_B;
+    constexpr bool INV = PASS < 2;
+    if constexpr (SHAPE >= 1) {
+        if (staged) return step_st_t<LOG_N, INV, PASS == 1, SHAPE, F>(ctx, a, st);
+    }
+    if (staged) return ZODA_ERR_UNSUPPORTED;
+    if constexpr (PASS == 1) return step2_t<LOG_N, true, SHAPE, F>(ctx, a, st);
+    else return step_t<LOG_N, INV, SHAPE, F>(ctx, a, st);
+}
+template <int LOG_N, int PASS>
+zoda_status ext_pass_shape(const zoda_ctx* ctx, int shape, const StepArgs& a, cudaStream_t st) {
+    const bool staged = shape & STEP_STAGED;
+    switch (shape & ~STEP_STAGED) {
+        case 1: return ext_pass_t<LOG_N, PASS, 1>(ctx, staged, a, st);
+        case 2: return ext_pass_t<LOG_N, PASS, 2>(ctx, staged, a, st);
+        case 3: return ext_pass_t<LOG_N, PASS, 3>(ctx, staged, a, st);
+        default: return ext_pass_t<LOG_N, PASS, 0>(ctx, staged, a, st);
+    }
+}
+template <int PASS>
+zoda_status ext_pass(const zoda_ctx* ctx, int log_n, int shape, const StepArgs& a, cudaStream_t st) {
+    switch (log_n) {
+        case 5: return ext_pass_shape<5, PASS>(ctx, shape, a, st);
+        case 6: return ext_pass_shape<6, PASS>(ctx, shape, a, st);
+        case 7: return ext_pass_shape<7, PASS>(ctx, shape, a, st);
+        default: return ZODA_ERR_UNSUPPORTED;
+    }
 }
 
 constexpr uint64_t NO_LIMIT = ~0ull;
@@ -135,7 +172,8 @@ zoda_status upload_table(zoda_ctx* ctx, int key, const std::vector<uint2>& h, co
 // base = omega_{2^ln}^c, split into [k1: base^k1 / n_k] (N1 entries) and
 // [k2: base^(N1*k2)] (N2 entries). Coset c's two tables sit at
 // *tabs + (c - 1) * (N1 + N2); built once per (L, ln). The extension is
-// ln = L + 1, c = 1 (base = g = omega_2S).
+// ln = L + 1, c = 1 (base = g = omega_2S); for it (L <= PIPE_MAX_LOG) the
+// product table [k2][k1] follows at *tabs + N1 + N2.
 zoda_status coset_mid_tables(zoda_ctx* ctx, int L, int ln, const uint2** tabs) {
     const int L1 = L / 2, L2 = L - L1;
     const uint32_t N1 = 1u << L1, N2 = 1u << L2;
@@ -149,6 +187,13 @@ zoda_status coset_mid_tables(zoda_ctx* ctx, int L, int ln, const uint2** tabs) {
             for (uint32_t k1 = 0, x = sinv; k1 < N1; k1++, x = mulmod_c(x, (uint32_t)base)) h.push_back(shoup_pair(x));
             const uint32_t step = powmod_c((uint32_t)base, N1);
             for (uint32_t k2 = 0, x = 1; k2 < N2; k2++, x = mulmod_c(x, step)) h.push_back(shoup_pair(x));
+        }
+        if (ln == L + 1 && L <= PIPE_MAX_LOG) {
+            // the extension's two factors as one table [k2][k1] = f1[k1] * f2[k2]:
+            // one product per coefficient in its block pass instead of two
+            const size_t f2 = N1;
+            for (uint32_t k2 = 0; k2 < N2; k2++)
+                for (uint32_t k1 = 0; k1 < N1; k1++) h.push_back(shoup_pair(mulmod_c(h[k1].x, h[f2 + k2].x)));
         }
         zoda_status s = b.ensure(h.size() * sizeof(uint2));
         if (s != ZODA_OK) return s;
@@ -230,7 +275,7 @@ zoda_status pipe_t(const zoda_ctx* ctx, const StepArgs pass[3], uint64_t cols, c
 
 template <int L1, int L2>
 zoda_status pipe_shape(const zoda_ctx* ctx, int shape, const StepArgs pass[3], uint64_t cols, cudaStream_t st) {
-    switch (shape) {
+    switch (shape & ~STEP_STAGED) {
         case 1: return pipe_t<L1, L2, 1>(ctx, pass, cols, st);
         case 2: return pipe_t<L1, L2, 2>(ctx, pass, cols, st);
         case 3: return pipe_t<L1, L2, 3>(ctx, pass, cols, st);
@@ -243,10 +288,10 @@ zoda_status pipe_shape(const zoda_ctx* ctx, int shape, const StepArgs pass[3], u
 // [S][cols] -> out [2S][cols]. The first pass writes the even rows (the input)
 // as it loads them; the odd rows hold the intermediate matrices. `tabs` =
 // coset_mid_tables(ctx, L, L + 1).
-int fourstep_shape(int radix, int ctas) {
+int fourstep_shape(int radix, int ctas, bool staged) {
     if (ctas <= 1) return 0;
-    if (radix == 16) return 1;
-    return ctas == 2 ? 2 : 3;
+    const int shape = radix == 16 ? 1 : ctas == 2 ? 2 : 3;
+    return shape | (staged ? STEP_STAGED : 0);
 }
 
 zoda_status long_extend(const zoda_ctx* ctx, int L, const uint2* tabs, const uint32_t* in, uint32_t* out,
@@ -275,8 +320,12 @@ zoda_status long_extend(const zoda_ctx* ctx, int L, const uint2* tabs, const uin
     // (N2, N1)), its twiddle omega_S^(k1 * m1)
     StepArgs& pm = pass[1];
     pm = plain_args(View{odd, op, N2 * op}, View{odd, op, N2 * op}, qpc, N1 * qpc);
-    pm.mid1 = FTab{cbtab, 0, 1};
-    pm.mid2 = FTab{ktab, 1, 0};
+    if (L <= PIPE_MAX_LOG) {
+        pm.mid1 = FTab{tabs + N1 + N2, (uint32_t)N1, 1};  // [k2][k1] products
+    } else {
+        pm.mid1 = FTab{cbtab, 0, 1};
+        pm.mid2 = FTab{ktab, 1, 0};
+    }
     pm.tw_log = L;
     // pass B of the NTT, in place: wide rows j2 of column block m1 -> odd row m1 + N2*m2
     StepArgs& pb = pass[2];
@@ -291,9 +340,14 @@ zoda_status long_extend(const zoda_ctx* ctx, int L, const uint2* tabs, const uin
             default: return ZODA_ERR_UNSUPPORTED;
         }
     }
-    if ((s = run_step(ctx, L1, true, pa, st, shape)) != ZODA_OK) return s;
-    if ((s = run_step2(ctx, L2, true, pm, st, shape)) != ZODA_OK) return s;
-    return run_step(ctx, L1, false, pb, st, shape);
+    if (L <= PIPE_MAX_LOG) {
+        if ((s = ext_pass<0>(ctx, L1, shape, pa, st)) != ZODA_OK) return s;
+        if ((s = ext_pass<1>(ctx, L2, shape, pm, st)) != ZODA_OK) return s;
+        return ext_pass<2>(ctx, L1, shape, pb, st);
+    }
+    if ((s = run_step(ctx, L1, true, pa, st)) != ZODA_OK) return s;
+    if ((s = run_step2(ctx, L2, true, pm, st)) != ZODA_OK) return s;
+    return run_step(ctx, L1, false, pb, st);
 }
 
 // Cosets c >= 1 of the encode for n_k = 2^lp > 4096 (general.cu copies coset 0,

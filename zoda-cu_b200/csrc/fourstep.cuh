@@ -67,6 +67,26 @@ struct StepArgs {
     unsigned long long* counter;  // or nullptr
 };
 
+// Features a pass may use, as compile-time flags: a pass instantiated without a
+// flag drops that feature's code and its runtime test (SF_ALL keeps every test).
+enum : int {
+    SF_PRE = 1,       // row pre-factors
+    SF_LIM_IN = 2,    // input row limit
+    SF_LIM_OUT = 4,   // output cut
+    SF_POST = 8,      // output factors
+    SF_TW = 16,       // output twiddle omega^(+-cb*k)
+    SF_SCALE = 64,    // output scale
+    SF_COPY = 128,    // copy of the loaded rows
+    SF_MID = 256,     // factors between the two transforms
+    SF_CNT = 512,     // count of nonzero high coefficients
+    SF_ALL = 1023,
+    // the extension's passes (long_extend): strided INTT with twiddle and even-row
+    // copy; block pass with the middle factors and twiddle; strided NTT
+    SF_EXT_A = SF_TW | SF_COPY,
+    SF_EXT_M = SF_MID | SF_TW,
+    SF_EXT_B = 0,
+};
+
 __device__ __forceinline__ Tw ftab_at(const FTab& f, uint32_t r, uint32_t cb) {
     const uint2 u = __ldg(f.tab + (r * f.rm + cb * f.cm));
     return Tw{u.x, u.y};
@@ -122,9 +142,17 @@ __device__ __forceinline__ void step_st(uint32_t* p, const V4& v) {
     else stg_stream_v4(p, v);
 }
 
+// Input row `row` of the quad exists (the quad is real and the row is inside the limit).
+template <int F = SF_ALL>
+__device__ __forceinline__ bool row_in(const StepArgs& a, const QuadPos& p, uint32_t row) {
+    if constexpr (F & SF_LIM_IN)
+        return p.active && (uint64_t)row * a.in_lim_rm + (uint64_t)p.cb * a.in_lim_cm < a.in_limit;
+    return p.active;
+}
+
 // Level 0 input: rows t + L0*j of the thread's quad, pre-factors applied, rows
 // past the limit (or with a zero factor) as zeros.
-template <class PL, bool LD_L2 = false>
+template <class PL, bool LD_L2 = false, int F = SF_ALL>
 __device__ __forceinline__ void step_load(V4* v, const StepArgs& a, const QuadPos& p, int t) {
     constexpr int R0 = 1 << PL::lr(0);
     constexpr int L0 = PL::S / R0;
@@ -132,19 +160,19 @@ __device__ __forceinline__ void step_load(V4* v, const StepArgs& a, const QuadPo
 #pragma unroll
     for (int j = 0; j < R0; j++) {
         const uint32_t row = (uint32_t)t + (uint32_t)L0 * j;
-        bool ld = p.active && (uint64_t)row * a.in_lim_rm + (uint64_t)p.cb * a.in_lim_cm < a.in_limit;
+        bool ld = row_in<F>(a, p, row);
         Tw f{1u, 0u};
-        if (a.pre.tab && ld) {
+        if ((F & SF_PRE) && a.pre.tab && ld) {
             f = ftab_at(a.pre, row, p.cb);
             ld = f.w != 0;
         }
         if (ld) {
             v[j] = step_ld<LD_L2>(src + (uint64_t)row * a.in.row_pitch);
-            if (a.copy.base)
+            if ((F & SF_COPY) && a.copy.base)
                 stg_stream_v4(a.copy.base + (uint64_t)p.cb * a.copy.cb_pitch + 4ull * p.qi +
                                   (uint64_t)row * a.copy.row_pitch,
                               v[j]);
-            if (a.pre.tab) mul4(v[j], f);
+            if ((F & SF_PRE) && a.pre.tab) mul4(v[j], f);
         } else {
             v[j] = V4{{0, 0, 0, 0}};
         }
@@ -152,15 +180,71 @@ __device__ __forceinline__ void step_load(V4* v, const StepArgs& a, const QuadPo
 }
 
 // Output k of the thread's quad: post factors, then the store (if in range).
-template <bool ST_KEEP = false>
+template <bool ST_KEEP = false, int F = SF_ALL>
 __device__ __forceinline__ void step_store(V4 x, const StepArgs& a, const QuadPos& p, uint32_t k,
                                            const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo) {
-    if (!p.active || (uint64_t)k * a.out_lim_rm + (uint64_t)p.cb * a.out_lim_cm >= a.out_limit) return;
-    if (a.post.tab) mul4(x, ftab_at(a.post, k, p.cb));
-    if (a.tw_log) mul_tw2d(x, p.cb * k, a.tw_log, a.tw_inv, tw, tw_lo);
-    if (a.use_scale) mul4(x, a.scale);
+    if (!p.active) return;
+    if constexpr (F & SF_LIM_OUT)
+        if ((uint64_t)k * a.out_lim_rm + (uint64_t)p.cb * a.out_lim_cm >= a.out_limit) return;
+    if ((F & SF_POST) && a.post.tab) mul4(x, ftab_at(a.post, k, p.cb));
+    if ((F & SF_TW) && a.tw_log) mul_tw2d(x, p.cb * k, a.tw_log, a.tw_inv, tw, tw_lo);
+    if ((F & SF_SCALE) && a.use_scale) mul4(x, a.scale);
     step_st<ST_KEEP>(a.out.base + (uint64_t)p.cb * a.out.cb_pitch + 4ull * p.qi + (uint64_t)k * a.out.row_pitch,
                      x);
+}
+
+// ---- staged loads: a tile's level-0 rows arrive by cp.async ---------------------
+// Each thread copies exactly the 16-byte slots it reads back later (rows t + L0*j
+// of its quad), so a thread's own cp.async.wait_group is the only wait the staged
+// data needs. cp.async.cg goes through L2 only, never a stale L1 line. Rows that
+// do not exist are zero-filled (source size 0) from a valid address.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Start the copies of tile `tile`'s level-0 rows into `stage` ([S][Q4] uint4 slots).
+template <class PL, int F = SF_ALL>
+__device__ __forceinline__ void step_prefetch(uint4* stage, const StepArgs& a, uint64_t tile, int q, int t) {
+    constexpr int R0 = 1 << PL::lr(0);
+    constexpr int L0 = PL::S / R0;
+    const QuadPos p(tile * PL::Q4 + q, a);
+    const uint32_t* src = a.in.base + (uint64_t)p.cb * a.in.cb_pitch + 4ull * p.qi;
+#pragma unroll
+    for (int j = 0; j < R0; j++) {
+        const uint32_t row = (uint32_t)t + (uint32_t)L0 * j;
+        const bool ld = row_in<F>(a, p, row);
+        cp_async16(stage + (size_t)row * PL::Q4 + q, ld ? src + (uint64_t)row * a.in.row_pitch : a.in.base, ld);
+    }
+}
+
+// Level 0 input from the stage: the copy of the loaded rows and the pre-factors as
+// step_load (a row with a zero pre-factor is loaded and multiplied to zero).
+template <class PL, int F = SF_ALL>
+__device__ __forceinline__ void step_consume(V4* v, const uint4* stage, const StepArgs& a, const QuadPos& p, int q,
+                                             int t) {
+    constexpr int R0 = 1 << PL::lr(0);
+    constexpr int L0 = PL::S / R0;
+#pragma unroll
+    for (int j = 0; j < R0; j++) {
+        const uint32_t row = (uint32_t)t + (uint32_t)L0 * j;
+        const uint4 u = stage[(size_t)row * PL::Q4 + q];
+        v[j] = V4{{u.x, u.y, u.z, u.w}};
+        if (((F & SF_COPY) && a.copy.base) || ((F & SF_PRE) && a.pre.tab)) {
+            const bool ld = row_in<F>(a, p, row);
+            if ((F & SF_COPY) && ld && a.copy.base)
+                stg_stream_v4(a.copy.base + (uint64_t)p.cb * a.copy.cb_pitch + 4ull * p.qi +
+                                  (uint64_t)row * a.copy.row_pitch,
+                              v[j]);
+            if ((F & SF_PRE) && ld && a.pre.tab) mul4(v[j], ftab_at(a.pre, row, p.cb));
+        }
+    }
 }
 
 // Launch shapes of the passes: level radix 2^LEPT, THREADS per CTA, MINB CTAs
@@ -177,11 +261,18 @@ struct StepShape {
     static constexpr int THREADS = SHAPE == 0 ? (LOG_N >= 9 ? 1024 : 512) : SHAPE == 2 ? 512 : 256;
     static constexpr int MINB = SHAPE == 0 ? 1 : SHAPE == 3 ? 4 : 2;
     using PL = ExtPlan<LOG_N, 0, LEPT, THREADS>;
+    // staged passes hold two tiles (the next one arriving, the current one, which
+    // also serves as the exchange buffer): CTAs per SM that fit 227 KB
+    static constexpr int MINB_ST_FIT = (int)(232448 / (2 * (PL::SMEM > 0 ? PL::SMEM : 1)));
+    static constexpr int MINB_ST = MINB_ST_FIT < MINB ? MINB_ST_FIT : MINB;
 };
 
 // One tile of a one-transform pass: N = 2^LOG_N points per virtual quad (INV:
 // inverse roots, unscaled) for the Q4 consecutive quads of tile `tile`.
-template <int LOG_N, bool INV, int SHAPE, bool LD_L2 = false, bool ST_KEEP = false>
+// STAGED: the level-0 rows are already in sm (step_prefetch), which then also
+// serves as the exchange buffer.
+template <int LOG_N, bool INV, int SHAPE, bool LD_L2 = false, bool ST_KEEP = false, bool STAGED = false,
+          int F = SF_ALL>
 __device__ __forceinline__ void step_tile(const StepArgs& a, uint64_t tile, uint4* sm, int tid,
                                           const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo) {
     using PL = typename StepShape<LOG_N, SHAPE>::PL;
@@ -189,7 +280,8 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, uint64_t tile, uint
     const int t = tid / PL::Q4;
     V4 v[PL::EPT];
     const QuadPos p(tile * PL::Q4 + q, a);
-    step_load<PL, LD_L2>(v, a, p, t);
+    if constexpr (STAGED) step_consume<PL, F>(v, sm, a, p, q, t);
+    else step_load<PL, LD_L2, F>(v, a, p, t);
     dif_levels<PL, 0, INV>(v, sm, t, q, tw);
     using LV = Level<PL, PL::lr(PL::NLEV - 1), PL::pre(PL::NLEV - 1)>;
 #pragma unroll
@@ -199,24 +291,24 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, uint64_t tile, uint
         for (int r = 0; r < LV::R; r++) {
             const uint32_t k =
                 digit_rev<PL, false>((blk << PL::lr(PL::NLEV - 1)) + (uint32_t)bitrev(r, PL::lr(PL::NLEV - 1)));
-            step_store<ST_KEEP>(v[g * LV::R + r], a, p, k, tw, tw_lo);
+            step_store<ST_KEEP, F>(v[g * LV::R + r], a, p, k, tw, tw_lo);
         }
     }
 }
 
 // One transform of N = 2^LOG_N points per virtual quad (INV: inverse roots,
 // unscaled), tiles of Q4 consecutive quads dealt round-robin.
-template <int LOG_N, bool INV, int SHAPE>
+template <int LOG_N, bool INV, int SHAPE, int F = SF_ALL>
 __global__ void __launch_bounds__(StepShape<LOG_N, SHAPE>::THREADS, StepShape<LOG_N, SHAPE>::MINB)
     k_step(const StepArgs a, uint64_t ntiles, const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo) {
     extern __shared__ uint4 sm[];
     for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
-        step_tile<LOG_N, INV, SHAPE>(a, tile, sm, threadIdx.x, tw, tw_lo);
+        step_tile<LOG_N, INV, SHAPE, false, false, false, F>(a, tile, sm, threadIdx.x, tw, tw_lo);
 }
 
 // The second transform's levels 1 .. NLEV-1 (mirrored radices, as ntt_levels in
 // extend.cuh, with either root direction); the last level stores every output.
-template <class PL, int l, bool INV2, bool ST_KEEP = false>
+template <class PL, int l, bool INV2, bool ST_KEEP = false, int F = SF_ALL>
 __device__ __forceinline__ void step2_levels(V4* v, uint4* sm, int t, int q, const Tw* tw, const Tw* tw_lo,
                                              const StepArgs& a, const QuadPos& p) {
     using LV = Level<PL, PL::nlr(l), PL::npre(l)>;
@@ -225,7 +317,7 @@ __device__ __forceinline__ void step2_levels(V4* v, uint4* sm, int t, int q, con
     if constexpr (l < PL::NLEV - 1) {
         LV::template twiddle_write<INV2>(v, sm, t, q, tw);
         __syncthreads();
-        step2_levels<PL, l + 1, INV2, ST_KEEP>(v, sm, t, q, tw, tw_lo, a, p);
+        step2_levels<PL, l + 1, INV2, ST_KEEP, F>(v, sm, t, q, tw, tw_lo, a, p);
     } else {
 #pragma unroll
         for (int g = 0; g < LV::G; g++) {
@@ -233,7 +325,7 @@ __device__ __forceinline__ void step2_levels(V4* v, uint4* sm, int t, int q, con
 #pragma unroll
             for (int r = 0; r < LV::R; r++) {
                 const uint32_t k = digit_rev<PL, true>((blk << PL::nlr(l)) + (uint32_t)bitrev(r, PL::nlr(l)));
-                step_store<ST_KEEP>(v[g * LV::R + r], a, p, k, tw, tw_lo);
+                step_store<ST_KEEP, F>(v[g * LV::R + r], a, p, k, tw, tw_lo);
             }
         }
     }
@@ -244,7 +336,8 @@ __device__ __forceinline__ void step2_levels(V4* v, uint4* sm, int t, int q, con
 // when INV2, both unscaled. mid(k, cb) = mid1(k, cb) * mid2(k, cb). With a
 // counter, the nonzero outputs k >= count_from of T1 (before mid) are added to
 // cnt (the decoder's consistency check).
-template <int LOG_N, bool INV1, bool INV2, int SHAPE, bool LD_L2 = false, bool ST_KEEP = false>
+template <int LOG_N, bool INV1, bool INV2, int SHAPE, bool LD_L2 = false, bool ST_KEEP = false,
+          bool STAGED = false, int F = SF_ALL>
 __device__ __forceinline__ void step2_tile(const StepArgs& a, uint64_t tile, uint4* sm, int tid,
                                            const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo,
                                            unsigned long long& cnt) {
@@ -253,7 +346,8 @@ __device__ __forceinline__ void step2_tile(const StepArgs& a, uint64_t tile, uin
     const int t = tid / PL::Q4;
     V4 v[PL::EPT];
     const QuadPos p(tile * PL::Q4 + q, a);
-    step_load<PL, LD_L2>(v, a, p, t);
+    if constexpr (STAGED) step_consume<PL, F>(v, sm, a, p, q, t);
+    else step_load<PL, LD_L2, F>(v, a, p, t);
     dif_levels<PL, 0, INV1>(v, sm, t, q, tw);
     // T1's last level: group g (block b = g*TPQ + t) holds outputs c0 + (S/R)*j at
     // v[g*R + bitrev(j)]; T2's first level (radix R over stride S/R) wants them in
@@ -272,11 +366,11 @@ __device__ __forceinline__ void step2_tile(const StepArgs& a, uint64_t tile, uin
         for (int j = 0; j < R; j++) {
             y[j] = v[g * R + bitrev(j, LR)];
             const uint32_t k = c0[g] + ((uint32_t)j << SH);
-            if (a.counter && p.active && k >= a.count_from)
+            if ((F & SF_CNT) && a.counter && p.active && k >= a.count_from)
 #pragma unroll
                 for (int e = 0; e < 4; e++) cnt += y[j].c[e] != 0;
-            if (a.mid1.tab) mul4(y[j], ftab_at(a.mid1, k, p.cb));
-            if (a.mid2.tab) mul4(y[j], ftab_at(a.mid2, k, p.cb));
+            if ((F & SF_MID) && a.mid1.tab) mul4(y[j], ftab_at(a.mid1, k, p.cb));
+            if ((F & SF_MID) && a.mid2.tab) mul4(y[j], ftab_at(a.mid2, k, p.cb));
         }
 #pragma unroll
         for (int j = 0; j < R; j++) v[g * R + j] = y[j];
@@ -298,24 +392,63 @@ __device__ __forceinline__ void step2_tile(const StepArgs& a, uint64_t tile, uin
             }
         }
         __syncthreads();
-        step2_levels<PL, 1, INV2, ST_KEEP>(v, sm, t, q, tw, tw_lo, a, p);
+        step2_levels<PL, 1, INV2, ST_KEEP, F>(v, sm, t, q, tw, tw_lo, a, p);
     } else {
 #pragma unroll
-        for (int r = 0; r < R; r++) step_store<ST_KEEP>(v[r], a, p, (uint32_t)bitrev(r, LR), tw, tw_lo);
+        for (int r = 0; r < R; r++) step_store<ST_KEEP, F>(v[r], a, p, (uint32_t)bitrev(r, LR), tw, tw_lo);
     }
 }
 
 // Two transforms per virtual quad with a factor between them (step2_tile), tiles
 // of Q4 consecutive quads dealt round-robin.
-template <int LOG_N, bool INV1, bool INV2, int SHAPE>
+template <int LOG_N, bool INV1, bool INV2, int SHAPE, int F = SF_ALL>
 __global__ void __launch_bounds__(StepShape<LOG_N, SHAPE>::THREADS, StepShape<LOG_N, SHAPE>::MINB)
     k_step2(const StepArgs a, uint64_t ntiles, const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo) {
     extern __shared__ uint4 sm[];
     const int tid = threadIdx.x;
     unsigned long long cnt = 0;
     for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
-        step2_tile<LOG_N, INV1, INV2, SHAPE>(a, tile, sm, tid, tw, tw_lo, cnt);
-    if (a.counter) {
+        step2_tile<LOG_N, INV1, INV2, SHAPE, false, false, false, F>(a, tile, sm, tid, tw, tw_lo, cnt);
+    if ((F & SF_CNT) && a.counter) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xFFFFFFFFu, cnt, o);
+        if ((tid & 31) == 0 && cnt) atomicAdd(a.counter, cnt);
+    }
+}
+
+// One pass (TWO: two transforms, T1 inverse when INV, T2 the other direction; else
+// one transform) with the next tile's rows copied in by cp.async while the
+// current tile computes. Shared memory holds two tiles; the current one is also
+// the exchange buffer, so a barrier at the top of each tile keeps the copies into
+// the other stage behind the previous tile's last exchange reads.
+template <int LOG_N, bool INV, bool TWO, int SHAPE, int F = SF_ALL>
+__global__ void __launch_bounds__(StepShape<LOG_N, SHAPE>::THREADS, StepShape<LOG_N, SHAPE>::MINB_ST)
+    k_step_st(const StepArgs a, uint64_t ntiles, const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo) {
+    using PL = typename StepShape<LOG_N, SHAPE>::PL;
+    static_assert(PL::SMEM > 0, "staged passes exchange through the stage");
+    extern __shared__ uint4 sm[];
+    constexpr size_t STG = PL::SMEM / sizeof(uint4);
+    const int tid = threadIdx.x;
+    const int q = tid % PL::Q4;
+    const int t = tid / PL::Q4;
+    unsigned long long cnt = 0;
+    uint64_t tile = blockIdx.x;
+    if (tile < ntiles) step_prefetch<PL, F>(sm, a, tile, q, t);
+    cp_async_commit();
+    for (int i = 0; tile < ntiles; tile += gridDim.x, i ^= 1) {
+        __syncthreads();  // the previous tile's exchange reads of the other stage are done
+        const uint64_t next = tile + gridDim.x;
+        if (next < ntiles) step_prefetch<PL, F>(sm + (i ^ 1) * STG, a, next, q, t);
+        cp_async_commit();
+        cp_async_wait<1>();  // this thread's rows of the current tile have landed
+        uint4* cur = sm + i * STG;
+        if constexpr (TWO)
+            step2_tile<LOG_N, INV, !INV, SHAPE, false, false, true, F>(a, tile, cur, tid, tw, tw_lo, cnt);
+        else
+            step_tile<LOG_N, INV, SHAPE, false, false, true, F>(a, tile, cur, tid, tw, tw_lo);
+    }
+    cp_async_wait<0>();
+    if (TWO && (F & SF_CNT) && a.counter) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xFFFFFFFFu, cnt, o);
         if ((tid & 31) == 0 && cnt) atomicAdd(a.counter, cnt);
@@ -377,12 +510,12 @@ __device__ __forceinline__ void pipe_pass(const PipeArgs& pa, uint32_t c, uint32
     if (x.copy.base) x.copy.base += off;
     if (c + 1 == pa.nchunks) x.qlim = pa.last_qlim;
     if constexpr (PH == 0) {
-        step_tile<L1, true, SHAPE, false, true>(x, tile, sm, tid, tw, tw_lo);
+        step_tile<L1, true, SHAPE, false, true, false, SF_EXT_A>(x, tile, sm, tid, tw, tw_lo);
     } else if constexpr (PH == 1) {
         unsigned long long cnt = 0;
-        step2_tile<L2, true, false, SHAPE, true, true>(x, tile, sm, tid, tw, tw_lo, cnt);
+        step2_tile<L2, true, false, SHAPE, true, true, false, SF_EXT_M>(x, tile, sm, tid, tw, tw_lo, cnt);
     } else {
-        step_tile<L1, false, SHAPE, true, false>(x, tile, sm, tid, tw, tw_lo);
+        step_tile<L1, false, SHAPE, true, false, false, SF_EXT_B>(x, tile, sm, tid, tw, tw_lo);
     }
 }
 

@@ -167,8 +167,10 @@ constexpr int PIPE_MAX_LOG = 14;
 zoda_status long_extend(const zoda_ctx* ctx, int L, const uint2* tabs, const uint32_t* in, uint32_t* out,
                         uint64_t cols, cudaStream_t st, bool odd_only = false, int shape = 0,
                         bool pipelined = false);
-// The four-step launch shape of a plan's (radix, ctas).
-int fourstep_shape(int radix, int ctas);
+// The four-step launch shape of a plan's (radix, ctas); staged adds STEP_STAGED (the
+// passes copy each next tile in by cp.async while the current one computes).
+constexpr int STEP_STAGED = 4;
+int fourstep_shape(int radix, int ctas, bool staged = false);
 // Smallest side (log2) the four-step plan covers.
 constexpr int FOURSTEP_MIN_LOG = 10;
 // Cosets c >= 1 of the encode of k data rows with n parity rows, n_k = next_pow2(k)
