@@ -46,9 +46,10 @@ __device__ __forceinline__ void bfly4(V4& a, V4& b, uint32_t w, uint32_t ws) {
 #pragma unroll
     for (int c = 0; c < 4; c++) dif_bfly(a.c[c], b.c[c], w, ws);
 }
+template <int LH = 0>
 __device__ __forceinline__ void bfly4_1(V4& a, V4& b) {
 #pragma unroll
-    for (int c = 0; c < 4; c++) dif_bfly1(a.c[c], b.c[c]);
+    for (int c = 0; c < 4; c++) dif_bfly1<((ZB_FREE_IMAD_MASK >> LH) & 1) != 0>(a.c[c], b.c[c]);
 }
 __device__ __forceinline__ void mul4(V4& a, const Tw t) {
 #pragma unroll
@@ -62,7 +63,7 @@ __device__ __forceinline__ void bfly_at(V4* x) {
     if constexpr ((J & h) == 0) {
         constexpr int e = J & (h - 1);
         if constexpr (e == 0) {
-            bfly4_1(x[J], x[J + h]);
+            bfly4_1<LH>(x[J], x[J + h]);
         } else {
             constexpr uint32_t w = root_pow(LH + 1, (uint32_t)e, INV);
             constexpr uint32_t ws = shoup(w);
@@ -89,6 +90,44 @@ __device__ __forceinline__ void stages(V4* x) {
 template <int LOG_R, bool INV>
 __device__ __forceinline__ void dft_dif(V4* x) {
     detail::stages<INV, LOG_R, LOG_R - 1>(x);
+}
+
+namespace detail {
+template <int LR, bool SKIP0, int I, class TwF>
+__device__ __forceinline__ void pair_twout(V4* x, const TwF& twf) {
+    constexpr int ka = bitrev(I, LR), kb = bitrev(I + 1, LR);
+    const Tw tb = twf.template get<kb>();
+    if constexpr (SKIP0 && ka == 0) {
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const uint32_t a = x[I].c[c], b = x[I + 1].c[c];
+            x[I].c[c] = add_mod(a, b);
+            x[I + 1].c[c] = mul_tw(a - b + P, tb.w, tb.ws);
+        }
+    } else {
+        const Tw ta = twf.template get<ka>();
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const uint32_t a = x[I].c[c], b = x[I + 1].c[c];
+            x[I].c[c] = mul_tw(a + b, ta.w, ta.ws);
+            x[I + 1].c[c] = mul_tw(a - b + P, tb.w, tb.ws);
+        }
+    }
+}
+template <int LR, bool SKIP0, class TwF, int... Is>
+__device__ __forceinline__ void last_stage_twout(V4* x, const TwF& twf, std::integer_sequence<int, Is...>) {
+    (pair_twout<LR, SKIP0, 2 * Is>(x, twf), ...);
+}
+}  // namespace detail
+
+// DIF DFT of size 2^LR whose last (twiddle-free) stage also multiplies output
+// k2 = bitrev(r) by twf.get<k2>(); a + b and a - b + p lie in [0, 2p), valid
+// Shoup inputs, so those sums are never reduced on their own. With SKIP0 the
+// output k2 = 0 has factor 1 and is only reduced.
+template <int LR, bool INV, bool SKIP0, class TwF>
+__device__ __forceinline__ void dft_dif_twout(V4* x, const TwF& twf) {
+    if constexpr (LR > 1) detail::stages<INV, LR, LR - 1, 1>(x);
+    detail::last_stage_twout<LR, SKIP0>(x, twf, std::make_integer_sequence<int, (1 << LR) / 2>{});
 }
 
 }  // namespace zb

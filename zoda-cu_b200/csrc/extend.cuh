@@ -93,6 +93,7 @@ __device__ __forceinline__ Tw tw_at(const Tw* __restrict__ tw, uint32_t e, int l
 // n1 + L*n2 (L = 2^LOGL); a group is (block, n1) and holds R = 2^LR slots.
 template <class PL, int LR, int PB>
 struct Level {
+    static constexpr int LRADIX = LR;
     static constexpr int R = 1 << LR;
     static constexpr int G = PL::EPT / R;
     static constexpr int LOGN = PL::LOG_S - PB;
@@ -128,6 +129,20 @@ struct Level {
                 V4 x = v[g * R + r];
                 if (k2 != 0) mul4(x, tw_at<INV>(tw, m * (uint32_t)k2, LOGN));
                 sm[(size_t)(b + ((uint32_t)k2 << LOGL)) * PL::Q4 + q] = make_uint4(x.c[0], x.c[1], x.c[2], x.c[3]);
+            }
+        }
+    }
+    // store output k2 = bitrev(r) of each group at slot base + L*k2 (its twiddle
+    // already applied)
+    __device__ static __forceinline__ void write(const V4* v, uint4* sm, int t, int q) {
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            const uint32_t b = base(gid(g, t));
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const V4& x = v[g * R + r];
+                sm[(size_t)(b + ((uint32_t)bitrev(r, LR) << LOGL)) * PL::Q4 + q] =
+                    make_uint4(x.c[0], x.c[1], x.c[2], x.c[3]);
             }
         }
     }

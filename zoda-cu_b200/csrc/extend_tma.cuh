@@ -176,44 +176,6 @@ struct KTw {  // a per-k2 table: factor for output k2 = K is p[K]
     }
 };
 
-namespace detail {
-template <int LR, bool SKIP0, int I, class TwF>
-__device__ __forceinline__ void pair_twout(V4* x, const TwF& twf) {
-    constexpr int ka = bitrev(I, LR), kb = bitrev(I + 1, LR);
-    const Tw tb = twf.template get<kb>();
-    if constexpr (SKIP0 && ka == 0) {
-#pragma unroll
-        for (int c = 0; c < 4; c++) {
-            const uint32_t a = x[I].c[c], b = x[I + 1].c[c];
-            x[I].c[c] = add_mod(a, b);
-            x[I + 1].c[c] = mul_tw(a - b + P, tb.w, tb.ws);
-        }
-    } else {
-        const Tw ta = twf.template get<ka>();
-#pragma unroll
-        for (int c = 0; c < 4; c++) {
-            const uint32_t a = x[I].c[c], b = x[I + 1].c[c];
-            x[I].c[c] = mul_tw(a + b, ta.w, ta.ws);
-            x[I + 1].c[c] = mul_tw(a - b + P, tb.w, tb.ws);
-        }
-    }
-}
-template <int LR, bool SKIP0, class TwF, int... Is>
-__device__ __forceinline__ void last_stage_twout(V4* x, const TwF& twf, std::integer_sequence<int, Is...>) {
-    (pair_twout<LR, SKIP0, 2 * Is>(x, twf), ...);
-}
-}  // namespace detail
-
-// DIF DFT of size 2^LR whose last (twiddle-free) stage also multiplies output
-// k2 = bitrev(r) by twf.get<k2>(); a + b and a - b + p lie in [0, 2p), valid
-// Shoup inputs, so those sums are never reduced on their own. With SKIP0 the
-// output k2 = 0 has factor 1 and is only reduced.
-template <int LR, bool INV, bool SKIP0, class TwF>
-__device__ __forceinline__ void dft_dif_twout(V4* x, const TwF& twf) {
-    if constexpr (LR > 1) detail::stages<INV, LR, LR - 1, 1>(x);
-    detail::last_stage_twout<LR, SKIP0>(x, twf, std::make_integer_sequence<int, (1 << LR) / 2>{});
-}
-
 // Level geometry (as ExtPlan): 2^PB blocks of N = 2^LOGN slots, slot = block*N |
 // n1 | (j << LOGL); the thread's group g is gid = g*TPQ + t.
 template <class TP, int LR, int PB>

@@ -93,11 +93,23 @@ __device__ __forceinline__ void dif_bfly(uint32_t& a, uint32_t& b, uint32_t w, u
 // ALU-light, these would otherwise be ALU-only and the ALU pipe would bind.
 // The multipliers 1 and 2^32-1 live in constant memory, which the assembler
 // cannot see through, so it keeps the IMADs instead of rewriting them as adds.
+// ZB_FREE_IMAD_MASK bit s set: the twiddle-free butterflies of DIF stages with
+// span 2^s use the IMAD form, else IADD3 (ALU) adds.
+#ifndef ZB_FREE_IMAD_MASK
+#define ZB_FREE_IMAD_MASK 0xFF
+#endif
 __constant__ uint32_t c_imad_one = 1u;
 __constant__ uint32_t c_imad_neg1 = 0xFFFFFFFFu;
+template <bool IMAD = true>
 __device__ __forceinline__ void dif_bfly1(uint32_t& a, uint32_t& b) {
-    const uint32_t u = a * c_imad_one + b;     // a + b, IMAD
-    const uint32_t d = b * c_imad_neg1 + a;    // a - b (mod 2^32), IMAD
+    uint32_t u, d;
+    if constexpr (IMAD) {
+        u = a * c_imad_one + b;     // a + b, IMAD
+        d = b * c_imad_neg1 + a;    // a - b (mod 2^32), IMAD
+    } else {
+        u = a + b;
+        d = a - b;
+    }
     a = __viaddmin_u32(u, 0u - P, u);             // min(u - p, u)
     b = __viaddmin_u32(d, P, d);                  // min(d + p, d)
 }
