@@ -253,6 +253,24 @@ zoda_status zoda_ctx_create(int device, zoda_ctx** out) {
             return fail(ZODA_ERR_NOMEM);
         }
     }
+    {
+        // compact roots of every size up to 8192 points, one size per run of entries
+        std::vector<Tw> cmp((size_t)2 << 13, Tw{1, shoup(1)});
+        for (int l = 0; l <= 13; l++) {
+            const uint32_t w = root_of_unity(l);
+            uint32_t cur = 1;
+            for (uint32_t j = 0; j < (1u << l); j++) {
+                cmp[(1u << l) + j] = Tw{cur, shoup(cur)};
+                cur = mulmod_c(cur, w);
+            }
+        }
+        if ((e = cudaMalloc(&c->tables.twc, cmp.size() * sizeof(Tw))) != cudaSuccess ||
+            (e = cudaMemcpy(c->tables.twc, cmp.data(), cmp.size() * sizeof(Tw), cudaMemcpyHostToDevice)) !=
+                cudaSuccess) {
+            set_last_error("cudaMalloc(twc)", e);
+            return fail(ZODA_ERR_NOMEM);
+        }
+    }
     if ((e = cudaMalloc(&c->d_err, sizeof(int))) != cudaSuccess || (e = cudaMemset(c->d_err, 0, sizeof(int))) != cudaSuccess) {
         set_last_error("cudaMalloc(err)", e);
         return fail(ZODA_ERR_NOMEM);
@@ -296,6 +314,7 @@ void zoda_ctx_destroy(zoda_ctx* c) {
     if (c->d_err) cudaFree(c->d_err);
     if (c->tables.tw) cudaFree(c->tables.tw);
     if (c->tables.tw_lo) cudaFree(c->tables.tw_lo);
+    if (c->tables.twc) cudaFree(c->tables.twc);
     if (c->tables.twist) cudaFree(c->tables.twist);
     if (c->tables.side) cudaFree(c->tables.side);
     for (auto& ev : c->ev)

@@ -30,6 +30,12 @@ inline unsigned pass_grid(const zoda_ctx* ctx, uint64_t ntiles, int minb) {
 }
 
 // One pass of any features (F = SF_ALL), or of a feature set the caller fixes.
+// Passes compiled with SF_FOLD read their level twiddles from the compact table.
+template <int F>
+inline const Tw* pass_tw(const zoda_ctx* ctx) {
+    return (F & SF_FOLD) ? ctx->tables.twc : ctx->tables.tw;
+}
+
 template <int LOG_N, bool INV, int SHAPE, int F = SF_ALL>
 zoda_status step_t(const zoda_ctx* ctx, const StepArgs& a, cudaStream_t st) {
     using SH = StepShape<LOG_N, SHAPE>;
@@ -40,7 +46,7 @@ zoda_status step_t(const zoda_ctx* ctx, const StepArgs& a, cudaStream_t st) {
         ZB_CUDA(cudaFuncSetAttribute(k_step<LOG_N, INV, SHAPE, F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)PL::SMEM));
     k_step<LOG_N, INV, SHAPE, F><<<pass_grid(ctx, ntiles, SH::MINB), PL::THREADS, PL::SMEM, st>>>(
-        a, ntiles, ctx->tables.tw, ctx->tables.tw_lo);
+        a, ntiles, pass_tw<F>(ctx), ctx->tables.tw_lo);
     ZB_CUDA(cudaGetLastError());
     return ZODA_OK;
 }
@@ -55,7 +61,7 @@ zoda_status step2_t(const zoda_ctx* ctx, const StepArgs& a, cudaStream_t st) {
         ZB_CUDA(cudaFuncSetAttribute(k_step2<LOG_N, INV1, !INV1, SHAPE, F>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PL::SMEM));
     k_step2<LOG_N, INV1, !INV1, SHAPE, F><<<pass_grid(ctx, ntiles, SH::MINB), PL::THREADS, PL::SMEM, st>>>(
-        a, ntiles, ctx->tables.tw, ctx->tables.tw_lo);
+        a, ntiles, pass_tw<F>(ctx), ctx->tables.tw_lo);
     ZB_CUDA(cudaGetLastError());
     return ZODA_OK;
 }
@@ -73,7 +79,7 @@ zoda_status step_st_t(const zoda_ctx* ctx, const StepArgs& a, cudaStream_t st) {
     ZB_CUDA(cudaFuncSetAttribute(k_step_st<LOG_N, INV, TWO, SHAPE, F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
     k_step_st<LOG_N, INV, TWO, SHAPE, F><<<pass_grid(ctx, ntiles, SH::MINB_ST), PL::THREADS, smem, st>>>(
-        a, ntiles, ctx->tables.tw, ctx->tables.tw_lo);
+        a, ntiles, pass_tw<F>(ctx), ctx->tables.tw_lo);
     ZB_CUDA(cudaGetLastError());
     return ZODA_OK;
 }
@@ -172,8 +178,10 @@ zoda_status upload_table(zoda_ctx* ctx, int key, const std::vector<uint2>& h, co
 // base = omega_{2^ln}^c, split into [k1: base^k1 / n_k] (N1 entries) and
 // [k2: base^(N1*k2)] (N2 entries). Coset c's two tables sit at
 // *tabs + (c - 1) * (N1 + N2); built once per (L, ln). The extension is
-// ln = L + 1, c = 1 (base = g = omega_2S); for it (L <= PIPE_MAX_LOG) the
-// product table [k2][k1] follows at *tabs + N1 + N2.
+// ln = L + 1, c = 1 (base = g = omega_2S); for it (L <= PIPE_MAX_LOG) three
+// tables of 2^L entries follow at *tabs + N1 + N2: the product table [k2][k1],
+// and the post-factor tables of the extension's INTT pass A ([i2][k1]) and of
+// its block pass ([k1][m1]).
 zoda_status coset_mid_tables(zoda_ctx* ctx, int L, int ln, const uint2** tabs) {
     const int L1 = L / 2, L2 = L - L1;
     const uint32_t N1 = 1u << L1, N2 = 1u << L2;
@@ -194,6 +202,16 @@ zoda_status coset_mid_tables(zoda_ctx* ctx, int L, int ln, const uint2** tabs) {
             const size_t f2 = N1;
             for (uint32_t k2 = 0; k2 < N2; k2++)
                 for (uint32_t k1 = 0; k1 < N1; k1++) h.push_back(shoup_pair(mulmod_c(h[k1].x, h[f2 + k2].x)));
+            // the output twiddles of its two transforms' first passes as post-factor
+            // tables: INTT pass A, [i2][k1] = omega_S^-(i2 * k1) (i2 < N2, k1 < N1);
+            // NTT pass A in the block pass, [k1][m1] = omega_S^(k1 * m1) (k1 < N1, m1 < N2)
+            const uint32_t wS = root_of_unity(L), wSi = powmod_c(wS, P - 2);
+            for (uint32_t i2 = 0; i2 < N2; i2++)
+                for (uint32_t k1 = 0, x = 1, st = powmod_c(wSi, i2); k1 < N1; k1++, x = mulmod_c(x, st))
+                    h.push_back(shoup_pair(x));
+            for (uint32_t k1 = 0; k1 < N1; k1++)
+                for (uint32_t m1 = 0, x = 1, st = powmod_c(wS, k1); m1 < N2; m1++, x = mulmod_c(x, st))
+                    h.push_back(shoup_pair(x));
         }
         zoda_status s = b.ensure(h.size() * sizeof(uint2));
         if (s != ZODA_OK) return s;
@@ -266,7 +284,7 @@ zoda_status pipe_t(const zoda_ctx* ctx, const StepArgs pass[3], uint64_t cols, c
     ZB_CUDA(cudaMemsetAsync(pa.counters, 0, cbytes, st));
     ZB_CUDA(cudaFuncSetAttribute(k_fourstep_pipe<L1, L2, SHAPE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)PS::SMEM));
-    k_fourstep_pipe<L1, L2, SHAPE><<<(unsigned)grid, PS::THREADS, PS::SMEM, st>>>(pa, ctx->tables.tw,
+    k_fourstep_pipe<L1, L2, SHAPE><<<(unsigned)grid, PS::THREADS, PS::SMEM, st>>>(pa, ctx->tables.twc,
                                                                                   ctx->tables.tw_lo);
     ZB_CUDA(cudaGetLastError());
     ZB_CUDA(cudaEventRecord(mc->pipe_done, st));
@@ -312,8 +330,13 @@ zoda_status long_extend(const zoda_ctx* ctx, int L, const uint2* tabs, const uin
     // loaded rows also go to the even rows
     StepArgs& pa = pass[0];
     pa = plain_args(View{const_cast<uint32_t*>(in), N2 * cols, cols}, View{odd, N2 * op, op}, qpc, N2 * qpc);
-    pa.tw_log = L;
-    pa.tw_inv = 1;
+    const uint64_t S = 1ull << L;
+    if (L <= PIPE_MAX_LOG) {
+        pa.post = FTab{tabs + N1 + N2 + S, 1, (uint32_t)N1};  // omega_S^-(i2 * k1) at [i2][k1]
+    } else {
+        pa.tw_log = L;
+        pa.tw_inv = 1;
+    }
     if (!odd_only) pa.copy = View{out, 2 * N2 * cols, 2 * cols};
     // block pass, in place: INTT pass B over i2 in block k1, the twist g^i / S
     // (g = omega_2S), NTT pass A over the block's coefficients (decomposition
@@ -321,12 +344,13 @@ zoda_status long_extend(const zoda_ctx* ctx, int L, const uint2* tabs, const uin
     StepArgs& pm = pass[1];
     pm = plain_args(View{odd, op, N2 * op}, View{odd, op, N2 * op}, qpc, N1 * qpc);
     if (L <= PIPE_MAX_LOG) {
-        pm.mid1 = FTab{tabs + N1 + N2, (uint32_t)N1, 1};  // [k2][k1] products
+        pm.mid1 = FTab{tabs + N1 + N2, (uint32_t)N1, 1};      // [k2][k1] products
+        pm.post = FTab{tabs + N1 + N2 + 2 * S, 1, (uint32_t)N2};  // omega_S^(k1 * m1) at [k1][m1]
     } else {
         pm.mid1 = FTab{cbtab, 0, 1};
         pm.mid2 = FTab{ktab, 1, 0};
+        pm.tw_log = L;
     }
-    pm.tw_log = L;
     // pass B of the NTT, in place: wide rows j2 of column block m1 -> odd row m1 + N2*m2
     StepArgs& pb = pass[2];
     pb = plain_args(View{odd, N2 * op, op}, View{odd, N2 * op, op}, qpc, N2 * qpc);

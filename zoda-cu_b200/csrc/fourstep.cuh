@@ -82,12 +82,15 @@ enum : int {
     SF_ALL = 1023,
     // SF_FOLD: every twiddle and factor that follows a DFT level is folded into the
     // level's last butterfly stage (dft_dif_twout), whose sums then skip their own
-    // reduction; with SF_MID it takes mid1 alone (mid2 unused) and no SF_CNT
+    // reduction. The pass then reads its level twiddles from the compact table
+    // (tw_at_c) passed in place of the omega_8192 table, takes its output twiddle
+    // as post-factors (no SF_TW), mid1 alone (mid2 unused), and no SF_CNT.
     SF_FOLD = 1024,
-    // the extension's passes (long_extend): strided INTT with twiddle and even-row
-    // copy; block pass with the middle factor and twiddle; strided NTT
-    SF_EXT_A = SF_TW | SF_COPY | SF_FOLD,
-    SF_EXT_M = SF_MID | SF_TW | SF_FOLD,
+    // the extension's passes (long_extend): strided INTT with its output twiddle
+    // (a post-factor table) and the even-row copy; block pass with the middle
+    // factor and its output twiddle; strided NTT
+    SF_EXT_A = SF_POST | SF_COPY | SF_FOLD,
+    SF_EXT_M = SF_MID | SF_POST | SF_FOLD,
     SF_EXT_B = SF_FOLD,
 };
 
@@ -277,46 +280,36 @@ struct StepShape {
 template <class PL, int l, bool MIR>
 using LvlOf = Level<PL, MIR ? PL::nlr(l) : PL::lr(l), MIR ? PL::npre(l) : PL::pre(l)>;
 
-// dft_dif_twout factor functors. LvlTw: a level's twiddle omega_{2^LOGN}^(+-m*k2).
+// omega_{2^logn}^(+-e) from the compact table: twc[2^logn + j] = omega_{2^logn}^j
+// for logn = 0 .. 13, so the roots of one size sit in consecutive lines.
+template <bool INV>
+__device__ __forceinline__ Tw tw_at_c(const Tw* __restrict__ twc, uint32_t e, int logn) {
+    const uint32_t mask = (1u << logn) - 1u;
+    const uint32_t idx = (1u << logn) | ((INV ? 0u - e : e) & mask);
+    const uint2 u = __ldg(reinterpret_cast<const uint2*>(twc) + idx);
+    return Tw{u.x, u.y};
+}
+
+// dft_dif_twout factor functors. LvlTw: a level's twiddle omega_{2^LOGN}^(+-m*k2)
+// from the compact table.
 template <bool INV, int LOGN>
 struct LvlTw {
-    const Tw* tw;
+    const Tw* twc;
     uint32_t m;
     template <int K>
     __device__ __forceinline__ Tw get() const {
-        return tw_at<INV>(tw, m * (uint32_t)K, LOGN);
+        return tw_at_c<INV>(twc, m * (uint32_t)K, LOGN);
     }
 };
-// The split of omega_{2^tw_log}^(+-e) over the two-level table: the exponent of
-// omega_{2^26}, whose high 13 bits index omega_8192 and low 13 bits omega_{2^26}.
-__device__ __forceinline__ uint32_t tw_exp26(uint32_t e, int tw_log, bool inv) {
-    uint32_t E = (e << (LOG_TWM - tw_log)) & TWM_MASK;
-    if (inv) E = (0u - E) & TWM_MASK;
-    return E;
-}
-// OutTw: a pass's output twiddle for output k = kb + (K << SH) of quad block cb,
-// the high-table factor (tw_log <= 13 needs nothing else; above, the caller
-// multiplies the low-table factor).
+// FacTw: a factor table's entry for output k = kb + (K << SH) of quad block cb
+// (the middle factor of the block pass, a pass's post-factors).
 template <int SH>
-struct OutTw {
-    const Tw* tw;
-    uint32_t cb, kb;
-    int tw_log, inv;
-    template <int K>
-    __device__ __forceinline__ Tw get() const {
-        const uint32_t E = tw_exp26(cb * (kb + ((uint32_t)K << SH)), tw_log, inv);
-        const uint2 u = __ldg(reinterpret_cast<const uint2*>(tw) + (E >> 13));
-        return Tw{u.x, u.y};
-    }
-};
-// MidTw: the middle factor mid1(c0 + (K << SH), cb).
-template <int SH>
-struct MidTw {
+struct FacTw {
     FTab f;
-    uint32_t c0, cb;
+    uint32_t kb, cb;
     template <int K>
     __device__ __forceinline__ Tw get() const {
-        return ftab_at(f, c0 + ((uint32_t)K << SH), cb);
+        return ftab_at(f, kb + ((uint32_t)K << SH), cb);
     }
 };
 
@@ -324,53 +317,37 @@ struct MidTw {
 // butterfly stage; returns with the last level's input in v. The write of level 0
 // waits for the previous tile's last exchange reads.
 template <class PL, int l, bool INV, bool MIR>
-__device__ __forceinline__ void fs_levels(V4* v, uint4* sm, int t, int q, const Tw* tw) {
+__device__ __forceinline__ void fs_levels(V4* v, uint4* sm, int t, int q, const Tw* twc) {
     using LV = LvlOf<PL, l, MIR>;
     if constexpr (l > 0) LV::read(v, sm, t, q);
     if constexpr (l < PL::NLEV - 1) {
 #pragma unroll
         for (int g = 0; g < LV::G; g++)
-            dft_dif_twout<LV::LRADIX, INV, true>(v + g * LV::R, LvlTw<INV, LV::LOGN>{tw, LV::n1(LV::gid(g, t))});
+            dft_dif_twout<LV::LRADIX, INV, true>(v + g * LV::R, LvlTw<INV, LV::LOGN>{twc, LV::n1(LV::gid(g, t))});
         if constexpr (l == 0) __syncthreads();
         LV::write(v, sm, t, q);
         __syncthreads();
-        fs_levels<PL, l + 1, INV, MIR>(v, sm, t, q, tw);
+        fs_levels<PL, l + 1, INV, MIR>(v, sm, t, q, twc);
     }
 }
 
-// The last level of a transform and the stores of its outputs, the output
-// twiddle (SF_TW) folded into the level's last butterfly stage.
+// The last level of a transform and the stores of its outputs, the post-factors
+// (SF_POST) folded into the level's last butterfly stage.
 template <class PL, bool INV, bool MIR, bool ST_KEEP, int F>
-__device__ __forceinline__ void fs_last_store(V4* v, int t, const StepArgs& a, const QuadPos& p,
-                                              const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo) {
+__device__ __forceinline__ void fs_last_store(V4* v, int t, const StepArgs& a, const QuadPos& p) {
+    static_assert(!(F & SF_TW), "folded passes take their output twiddle as post-factors");
     using LV = LvlOf<PL, PL::NLEV - 1, MIR>;
     constexpr int LR = LV::LRADIX;
     constexpr int SH = PL::LOG_S - LR;
 #pragma unroll
     for (int g = 0; g < LV::G; g++) {
-        const uint32_t blk = LV::gid(g, t);
-        const uint32_t kb = digit_rev<PL, MIR>(blk << LR);
-        if constexpr (F & SF_TW) {
-            if (a.tw_log) dft_dif_twout<LR, INV, false>(v + g * LV::R, OutTw<SH>{tw, p.cb, kb, a.tw_log, a.tw_inv});
-            else dft_dif<LR, INV>(v + g * LV::R);
-        } else {
-            dft_dif<LR, INV>(v + g * LV::R);
-        }
+        const uint32_t kb = digit_rev<PL, MIR>(LV::gid(g, t) << LR);
+        if constexpr (F & SF_POST) dft_dif_twout<LR, INV, false>(v + g * LV::R, FacTw<SH>{a.post, kb, p.cb});
+        else dft_dif<LR, INV>(v + g * LV::R);
 #pragma unroll
-        for (int r = 0; r < LV::R; r++) {
-            const uint32_t k = kb + ((uint32_t)bitrev(r, LR) << SH);
-            V4 x = v[g * LV::R + r];
-            if constexpr (F & SF_TW) {
-                if (a.tw_log > LOG_TW) {  // the low-table factor of a twiddle above 8192 points
-                    const uint32_t lo = tw_exp26(p.cb * k, a.tw_log, a.tw_inv) & 8191u;
-                    if (lo) {
-                        const uint2 u = __ldg(reinterpret_cast<const uint2*>(tw_lo) + lo);
-                        mul4(x, Tw{u.x, u.y});
-                    }
-                }
-            }
-            step_store<ST_KEEP, F & ~SF_TW>(x, a, p, k, tw, tw_lo);
-        }
+        for (int r = 0; r < LV::R; r++)
+            step_store<ST_KEEP, F & ~SF_POST>(v[g * LV::R + r], a, p, kb + ((uint32_t)bitrev(r, LR) << SH), nullptr,
+                                              nullptr);
     }
 }
 
@@ -390,8 +367,8 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, uint64_t tile, uint
     if constexpr (STAGED) step_consume<PL, F>(v, sm, a, p, q, t);
     else step_load<PL, LD_L2, F>(v, a, p, t);
     if constexpr (F & SF_FOLD) {
-        fs_levels<PL, 0, INV, false>(v, sm, t, q, tw);
-        fs_last_store<PL, INV, false, ST_KEEP, F>(v, t, a, p, tw, tw_lo);
+        fs_levels<PL, 0, INV, false>(v, sm, t, q, tw);  // tw: the compact table
+        fs_last_store<PL, INV, false, ST_KEEP, F>(v, t, a, p);
         return;
     }
     dif_levels<PL, 0, INV>(v, sm, t, q, tw);
@@ -473,13 +450,13 @@ __device__ __forceinline__ void step2_tile(const StepArgs& a, uint64_t tile, uin
         for (int g = 0; g < G; g++) {
             c0[g] = digit_rev<PL, false>((uint32_t)(g * PL::TPQ + t) << LR);
             // T1's last level with the middle factor of output c0 + (S/R) k2 folded in
-            if constexpr (F & SF_MID) dft_dif_twout<LR, INV1, false>(v + g * R, MidTw<SH>{a.mid1, c0[g], p.cb});
+            if constexpr (F & SF_MID) dft_dif_twout<LR, INV1, false>(v + g * R, FacTw<SH>{a.mid1, c0[g], p.cb});
             else dft_dif<LR, INV1>(v + g * R);
             V4 y[R];
 #pragma unroll
             for (int j = 0; j < R; j++) y[j] = v[g * R + bitrev(j, LR)];
             // T2 level 0 (radix R over stride S/R, group n1 = c0) with its twiddles
-            dft_dif_twout<LR, INV2, true>(y, LvlTw<INV2, PL::LOG_S>{tw, c0[g]});
+            dft_dif_twout<LR, INV2, true>(y, LvlTw<INV2, PL::LOG_S>{tw, c0[g]});  // tw: compact
 #pragma unroll
             for (int j = 0; j < R; j++) v[g * R + j] = y[j];
         }
@@ -494,7 +471,7 @@ __device__ __forceinline__ void step2_tile(const StepArgs& a, uint64_t tile, uin
             }
         __syncthreads();
         fs_levels<PL, 1, INV2, true>(v, sm, t, q, tw);
-        fs_last_store<PL, INV2, true, ST_KEEP, F>(v, t, a, p, tw, tw_lo);
+        fs_last_store<PL, INV2, true, ST_KEEP, F>(v, t, a, p);
         return;
     }
     dif_levels<PL, 0, INV1>(v, sm, t, q, tw);

@@ -67,6 +67,7 @@ struct DevBuf {
 struct Tables {
     Tw* tw = nullptr;
     Tw* tw_lo = nullptr;  // omega_{2^26}^j, j in [0, 8192): with tw, every 2^26-th root of unity
+    Tw* twc = nullptr;    // compact roots: twc[2^l + j] = omega_{2^l}^j, l = 0 .. 13
     Tw* twist = nullptr;
     // per-side level tables of the TMA-staged kernels (log2 side 5..12), one buffer
     Tw* side = nullptr;
