@@ -727,17 +727,32 @@ def workload_config(side: int) -> dict:
 
 
 def launches_per_step(side: int, plan: dict | None) -> int:
-    """Kernels zoda_extend_device launches per square: the four-step plan (and every side above
-    4096) runs three passes, the single-pass kernels one."""
-    if side > 4096 or (plan and plan.get("impl") == 3):
+    """Kernels zoda_extend_device launches per square: the four-step plan runs three passes, as
+    three launches or (blocked 1) one pipelined launch; every side above 4096 three launches; the
+    single-pass kernels one."""
+    if side > 4096:
         return 3
+    if plan and plan.get("impl") == 3:
+        return 1 if plan.get("blocked") else 3
     return 1
 
 
 def plan_kernels(side: int, plan: dict | None) -> str:
+    if plan and plan.get("impl") == 3 and plan.get("blocked") and side <= 4096:
+        return ("k_fourstep_pipe (the three four-step passes, strided INTT, block INTT+twist+NTT and "
+                "strided NTT, column chunk by column chunk in one persistent launch)")
     if side > 4096 or (plan and plan.get("impl") == 3):
-        return "k_step / k_step2 (three four-step passes: strided INTT, block INTT+twist+NTT, strided NTT)"
+        staged = " with cp.async-staged tiles" if plan and plan.get("sched") else ""
+        return ("k_step / k_step2 (three four-step passes: strided INTT, block INTT+twist+NTT, strided NTT)"
+                + staged)
     return kernel_name(side, plan)
+
+
+def traffic_key(side: int, plan: dict | None) -> str:
+    """profiles/traffic.json key of the kernel(s) one step runs."""
+    if plan and plan.get("impl") == 3:
+        return f"k_extend_side{side}_fourstep" + ("_pipe" if plan.get("blocked") else "")
+    return f"k_extend_side{side}"
 
 
 def measure_side(ctx, side: int, steps: int, warmup: int, world: int, sampler=None, tune_it: bool = True,
@@ -762,8 +777,7 @@ def measure_side(ctx, side: int, steps: int, warmup: int, world: int, sampler=No
         "clocks": clocks, "output_check": check,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": round(achieved / peaks["hbm_gbs"], 4),
-                     "traffic": ncu_traffic(f"k_extend_side{side}" + ("_fourstep" if launches_per_step(side, plan) == 3
-                                                                       else "")),
+                     "traffic": ncu_traffic(traffic_key(side, plan)),
                      "peak_source": peaks["source"], "kernel": plan_kernels(side, plan),
                      "launches_per_step": launches_per_step(side, plan), "alg_bytes_per_step": alg_bytes},
         "e2e": {"value": round(job_rate(world, side, e2e_max, 1), 3), "unit": "Gb/s",

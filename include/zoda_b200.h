@@ -110,9 +110,10 @@ typedef struct zoda_plan {
     int32_t impl;     /* ZODA_IMPL_DIRECT, ZODA_IMPL_TMA (k >= 32) or ZODA_IMPL_FOURSTEP
                          (1024 <= k <= 4096)                                          */
     int32_t sched;    /* direct kernel: the leftover radix at the INTT's last level (0)
-                         or its first level (1). FOURSTEP with ctas 2 or 4 and blocked 0:
-                         1 = each pass copies its next tile into shared memory by
-                         cp.async while the current one computes                      */
+                         or its first level (1). FOURSTEP with ctas 2 or 4: 1 = tiles
+                         are copied into shared memory by cp.async while the previous
+                         one computes (each pass's next tile; in the chunked launch,
+                         the next pass-A tile)                                        */
     int32_t l2_promo; /* TMA kernel: L2 promotion of tile loads, 0 none, 1 64 B,
                          2 128 B, 3 256 B                                              */
     int32_t blocked;  /* 0 = CTA i takes tiles i, i + grid, ...; 1 = one contiguous run.

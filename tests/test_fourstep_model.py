@@ -151,7 +151,7 @@ def pipe_geometry(L: int, q4a: int, q4m: int, grid: int, cols: int) -> dict:
     nch = -(-quads // cq)
     tiles = [N2 * cq // q4a, N1 * cq // q4m, N2 * cq // q4a]
     per_round = sum(tiles)
-    depth = max(1, -(-(2 * 2 * grid) // per_round))
+    depth = max(1, -(-(2 * 3 * grid) // per_round))
     return dict(cq=cq, nch=nch, tiles=tiles, per_round=per_round, depth=depth,
                 last_qlim=quads - (nch - 1) * cq, total=(nch + 2 * depth) * per_round)
 
@@ -171,7 +171,7 @@ def pipe_decode(item: int, g: dict):
 
 def model_extend_pipelined(data: np.ndarray, q4a: int, q4m: int, grid: int, seed: int) -> np.ndarray:
     """k_fourstep_pipe: the passes of long_extend as tiles of (chunk, pass), dealt in the
-    kernel's order to `grid` CTAs that each hold one item and the next one drawn, and
+    kernel's order to `grid` CTAs that each hold one item and the two drawn after it, and
     finished in a random order among those whose dependencies are met (a pass-B or block
     tile waits for every tile of the chunk's previous pass). Fails on a deadlock, a tile
     run twice or missed, or a tile run before its dependencies."""
@@ -209,9 +209,13 @@ def model_extend_pipelined(data: np.ndarray, q4a: int, q4m: int, grid: int, seed
         counter += 1
         return counter - 1
 
-    ctas = [[draw(), None] for _ in range(grid)]  # [current, drawn next]
+    # [current, next, the one after]: the kernel draws two items up front and, at the top
+    # of every item, the one after next (before it waits on the current one's dependencies)
+    ctas = [[draw(), draw()] for _ in range(grid)]
+    for cta in ctas:
+        cta.append(draw())
     while True:
-        live = [k for k, (it, _) in enumerate(ctas) if it < g["total"]]
+        live = [k for k, cta in enumerate(ctas) if cta[0] < g["total"]]
         if not live:
             break
         ready = []
@@ -221,8 +225,7 @@ def model_extend_pipelined(data: np.ndarray, q4a: int, q4m: int, grid: int, seed
                 ready.append(k)
         assert ready, "deadlock: every CTA waits"
         k = ready[rng.integers(len(ready))]
-        item = ctas[k][0]
-        ctas[k][1] = draw()
+        item, nxt, after = ctas[k]
         ph, c, j = pipe_decode(item, g)
         if c is not None:
             assert (ph, c, j) not in ran
@@ -232,7 +235,7 @@ def model_extend_pipelined(data: np.ndarray, q4a: int, q4m: int, grid: int, seed
             model_pass(a)
             if ph < 2:
                 done[ph][c] += 1
-        ctas[k] = [ctas[k][1], None]
+        ctas[k] = [nxt, after, draw()]
     assert len(ran) == g["nch"] * sum(g["tiles"])
     return out.reshape(2 * S, cols).astype(np.uint32)
 
@@ -395,5 +398,5 @@ def test_pipe_geometry_limits():
     # the kernel's item counter is 32-bit: the host keeps every draw below 2^31
     for L, q4a, q4m in ((10, 256, 256), (12, 128, 128), (12, 32, 32), (14, 64, 64)):
         g = pipe_geometry(L, q4a, q4m, 592, 1 << 26)
-        assert g["total"] + 2 * 592 < 1 << 31
+        assert g["total"] + 3 * 592 < 1 << 31
         assert all(t * q for t, q in zip(g["tiles"], (q4a, q4m, q4a)))

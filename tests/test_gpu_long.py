@@ -132,9 +132,10 @@ FOURSTEP_SHAPES = [(16, 1), (16, 2), (8, 2), (8, 4)]
 
 
 # plan forms: (sched, blocked) = three launches, three staged launches (cp.async
-# prefetch of each next tile), one pipelined launch
-FORMS = {"three-launches": (0, 0), "staged": (1, 0), "pipelined": (0, 1)}
-FOURSTEP_PLANS = [(f, r, c) for f in FORMS for r, c in FOURSTEP_SHAPES if not (f == "staged" and c == 1)]
+# prefetch of each next tile), one pipelined launch, one pipelined launch with the
+# next pass-A tile staged
+FORMS = {"three-launches": (0, 0), "staged": (1, 0), "pipelined": (0, 1), "staged-pipelined": (1, 1)}
+FOURSTEP_PLANS = [(f, r, c) for f in FORMS for r, c in FOURSTEP_SHAPES if not (FORMS[f][0] == 1 and c == 1)]
 
 
 @pytest.mark.parametrize("side", [1024, 2048, 4096])

@@ -93,15 +93,15 @@ std::vector<zoda_plan> candidates(int ls) {
                     }
     }
     // three four-step passes, in each launch shape: three launches over the square
-    // (blocked 0), the same with each next tile staged by cp.async (sched 1), or one
-    // launch that runs them column chunk by column chunk (blocked 1)
-    for (int form = 0; form < 3 && ls >= FOURSTEP_MIN_LOG; form++)
+    // (blocked 0) or one launch that runs them column chunk by column chunk
+    // (blocked 1), each with or without tiles staged by cp.async (sched 1)
+    for (int form = 0; form < 4 && ls >= FOURSTEP_MIN_LOG; form++)
         for (const auto& rc : {std::pair<int, int>{16, 1}, {16, 2}, {8, 2}, {8, 4}}) {
-            if (form == 1 && rc.second == 1) continue;
-            const int blocked = form == 2;
+            if ((form & 1) && rc.second == 1) continue;
+            const int blocked = form >= 2;
             zoda_plan p = d;
             p.impl = ZODA_IMPL_FOURSTEP;
-            p.sched = form == 1;
+            p.sched = form & 1;
             p.l2_promo = 3;
             p.blocked = blocked;
             p.stagger = 1;

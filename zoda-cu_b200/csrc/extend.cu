@@ -131,8 +131,7 @@ zoda_status check_plan(int log_s, const zoda_plan& p) {
             (p.radix == 8 && p.ctas <= 1))
             return ZODA_ERR_ARG;
         // sched 1: staged passes, which exist for the shapes of 2 and 4 CTAs per SM
-        // and the three-launch form
-        if (p.sched == 1 && (p.ctas <= 1 || p.blocked)) return ZODA_ERR_ARG;
+        if (p.sched == 1 && p.ctas <= 1) return ZODA_ERR_ARG;
     }
     if (p.sched < 0 || p.sched > 1 || p.l2_promo < 0 || p.l2_promo > 3 || p.blocked < 0 || p.blocked > 1 ||
         p.stagger < 0 || p.stagger > 3 || (p.radix != 16 && p.radix != 8))

@@ -245,7 +245,7 @@ zoda_status long_cols_ntt(const zoda_ctx* ctx, uint32_t* B, uint32_t* A, int L, 
 
 // The same three passes in one persistent launch, column chunk by column chunk
 // (k_fourstep_pipe), so each chunk's intermediate stays in L2 between its passes.
-template <int L1, int L2, int SHAPE>
+template <int L1, int L2, int SHAPE, bool STAGE>
 zoda_status pipe_t(const zoda_ctx* ctx, const StepArgs pass[3], uint64_t cols, cudaStream_t st) {
     using PS = PipeShape<L1, L2, SHAPE>;
     using PA = typename PS::A::PL;
@@ -263,14 +263,18 @@ zoda_status pipe_t(const zoda_ctx* ctx, const StepArgs pass[3], uint64_t cols, c
     pa.chunk_u32 = 4ull * PS::CQ;
     pa.nchunks = (uint32_t)nch;
     pa.last_qlim = (uint32_t)(quads - (nch - 1) * PS::CQ);
-    const uint64_t grid = (uint64_t)ctx->sm_count * PS::MINB;
+    constexpr int minb = STAGE ? PS::MINB_ST : PS::MINB;
+    static_assert(minb >= 1, "the CTA's buffers fit one SM");
+    constexpr size_t smem = (STAGE ? 2 : 1) * PS::SMEM;
+    const uint64_t grid = (uint64_t)ctx->sm_count * minb;
     const uint64_t per_round = (uint64_t)pa.tiles[0] + pa.tiles[1] + pa.tiles[2];
     // depth: enough rounds between a chunk's passes that its earlier tiles are done
-    // before the later ones are dealt (twice the items the CTAs hold at once)
-    uint64_t depth = (2 * 2 * grid + per_round - 1) / per_round;
+    // before the later ones are dealt (twice the items the CTAs hold at once: the
+    // current one and the two drawn ahead)
+    uint64_t depth = (2 * 3 * grid + per_round - 1) / per_round;
     if (depth < 1) depth = 1;
     pa.depth = (uint32_t)depth;
-    if (nch > (1u << 30) || (nch + 2 * depth) * per_round + 2 * grid >= (1ull << 31)) return ZODA_ERR_UNSUPPORTED;
+    if (nch > (1u << 30) || (nch + 2 * depth) * per_round + 3 * grid >= (1ull << 31)) return ZODA_ERR_UNSUPPORTED;
     zoda_ctx* mc = const_cast<zoda_ctx*>(ctx);  // the pipeline's counters and ordering event
     std::lock_guard<std::mutex> lock(mc->pipe_mu);
     const size_t cbytes = (size_t)(1 + 2 * nch) * sizeof(uint32_t);
@@ -282,10 +286,10 @@ zoda_status pipe_t(const zoda_ctx* ctx, const StepArgs pass[3], uint64_t cols, c
     // launches on other streams share the counters: each waits for the one before
     ZB_CUDA(cudaStreamWaitEvent(st, mc->pipe_done, 0));
     ZB_CUDA(cudaMemsetAsync(pa.counters, 0, cbytes, st));
-    ZB_CUDA(cudaFuncSetAttribute(k_fourstep_pipe<L1, L2, SHAPE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)PS::SMEM));
-    k_fourstep_pipe<L1, L2, SHAPE><<<(unsigned)grid, PS::THREADS, PS::SMEM, st>>>(pa, ctx->tables.twc,
-                                                                                  ctx->tables.tw_lo);
+    ZB_CUDA(cudaFuncSetAttribute(k_fourstep_pipe<L1, L2, SHAPE, STAGE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+    k_fourstep_pipe<L1, L2, SHAPE, STAGE><<<(unsigned)grid, PS::THREADS, smem, st>>>(pa, ctx->tables.twc,
+                                                                                    ctx->tables.tw_lo);
     ZB_CUDA(cudaGetLastError());
     ZB_CUDA(cudaEventRecord(mc->pipe_done, st));
     return ZODA_OK;
@@ -293,11 +297,12 @@ zoda_status pipe_t(const zoda_ctx* ctx, const StepArgs pass[3], uint64_t cols, c
 
 template <int L1, int L2>
 zoda_status pipe_shape(const zoda_ctx* ctx, int shape, const StepArgs pass[3], uint64_t cols, cudaStream_t st) {
+    const bool staged = shape & STEP_STAGED;
     switch (shape & ~STEP_STAGED) {
-        case 1: return pipe_t<L1, L2, 1>(ctx, pass, cols, st);
-        case 2: return pipe_t<L1, L2, 2>(ctx, pass, cols, st);
-        case 3: return pipe_t<L1, L2, 3>(ctx, pass, cols, st);
-        default: return pipe_t<L1, L2, 0>(ctx, pass, cols, st);
+        case 1: return staged ? pipe_t<L1, L2, 1, true>(ctx, pass, cols, st) : pipe_t<L1, L2, 1, false>(ctx, pass, cols, st);
+        case 2: return staged ? pipe_t<L1, L2, 2, true>(ctx, pass, cols, st) : pipe_t<L1, L2, 2, false>(ctx, pass, cols, st);
+        case 3: return staged ? pipe_t<L1, L2, 3, true>(ctx, pass, cols, st) : pipe_t<L1, L2, 3, false>(ctx, pass, cols, st);
+        default: return staged ? ZODA_ERR_UNSUPPORTED : pipe_t<L1, L2, 0, false>(ctx, pass, cols, st);
     }
 }
 

@@ -626,17 +626,26 @@ __device__ __forceinline__ bool pipe_wait_count(const uint32_t* p, uint32_t need
     return false;
 }
 
-template <int PH, int L1, int L2, int SHAPE>
-__device__ __forceinline__ void pipe_pass(const PipeArgs& pa, uint32_t c, uint32_t tile, uint4* sm, int tid,
-                                          const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo) {
+// Chunk c's view of pass PH.
+template <int PH>
+__device__ __forceinline__ StepArgs pipe_args(const PipeArgs& pa, uint32_t c) {
     StepArgs x = pa.pass[PH];
     const uint64_t off = (uint64_t)c * pa.chunk_u32;
     x.in.base += off;
     x.out.base += off;
     if (x.copy.base) x.copy.base += off;
     if (c + 1 == pa.nchunks) x.qlim = pa.last_qlim;
+    return x;
+}
+
+// STAGED0: pass-A tiles arrive staged in sm (step_prefetch); the other passes read
+// what this launch wrote straight from L2.
+template <int PH, int L1, int L2, int SHAPE, bool STAGED0>
+__device__ __forceinline__ void pipe_pass(const PipeArgs& pa, uint32_t c, uint32_t tile, uint4* sm, int tid,
+                                          const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo) {
+    const StepArgs x = pipe_args<PH>(pa, c);
     if constexpr (PH == 0) {
-        step_tile<L1, true, SHAPE, false, true, false, SF_EXT_A>(x, tile, sm, tid, tw, tw_lo);
+        step_tile<L1, true, SHAPE, false, true, STAGED0, SF_EXT_A>(x, tile, sm, tid, tw, tw_lo);
     } else if constexpr (PH == 1) {
         unsigned long long cnt = 0;
         step2_tile<L2, true, false, SHAPE, true, true, false, SF_EXT_M>(x, tile, sm, tid, tw, tw_lo, cnt);
@@ -653,69 +662,113 @@ struct PipeShape {
     static constexpr int THREADS = A::THREADS, MINB = A::MINB;
     static constexpr size_t SMEM = A::PL::SMEM > M::PL::SMEM ? A::PL::SMEM : M::PL::SMEM;
     static constexpr uint32_t CQ = A::PL::Q4 > M::PL::Q4 ? A::PL::Q4 : M::PL::Q4;  // quads per chunk
+    // staged: two tile buffers
+    static constexpr int MINB_ST_FIT = (int)(232448 / (2 * SMEM));
+    static constexpr int MINB_ST = MINB_ST_FIT < MINB ? MINB_ST_FIT : MINB;
 };
 
-template <int L1, int L2, int SHAPE>
-__global__ void __launch_bounds__(PipeShape<L1, L2, SHAPE>::THREADS, PipeShape<L1, L2, SHAPE>::MINB)
+// An item's pass, chunk (-1 or past the last: an empty item) and tile in the chunk.
+struct PipeItem {
+    int ph;
+    int64_t c;
+    uint32_t j;
+};
+__device__ __forceinline__ PipeItem pipe_decode(const PipeArgs& pa, uint32_t item, uint32_t per_round) {
+    const uint32_t r = item / per_round;
+    uint32_t j = item - r * per_round;
+    if (j < pa.tiles[0]) return PipeItem{0, (int64_t)r, j};
+    j -= pa.tiles[0];
+    if (j < pa.tiles[1]) return PipeItem{1, (int64_t)r - pa.depth, j};
+    return PipeItem{2, (int64_t)r - 2 * (int64_t)pa.depth, j - pa.tiles[1]};
+}
+
+// STAGE: two tile buffers; every CTA knows its next item one tile ahead, and when
+// that item is a pass-A tile (no dependencies) its rows are copied in by cp.async
+// while the current item computes. Items alternate buffers; the barrier at the top
+// of each item keeps the copies behind the previous item's last reads.
+template <int L1, int L2, int SHAPE, bool STAGE>
+__global__ void __launch_bounds__(PipeShape<L1, L2, SHAPE>::THREADS,
+                                  STAGE ? PipeShape<L1, L2, SHAPE>::MINB_ST : PipeShape<L1, L2, SHAPE>::MINB)
     k_fourstep_pipe(const __grid_constant__ PipeArgs pa, const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo) {
+    using PS = PipeShape<L1, L2, SHAPE>;
+    using PLA = typename PS::A::PL;
+    constexpr size_t BUF = PS::SMEM / sizeof(uint4);
     extern __shared__ uint4 sm[];
-    __shared__ uint32_t s_item;
+    __shared__ uint32_t s_item, s_next[2];  // s_next: a ring, so one barrier per item covers its reads
     __shared__ int s_fail;
     const int tid = threadIdx.x;
     const uint32_t per_round = pa.tiles[0] + pa.tiles[1] + pa.tiles[2];
     const uint32_t total = (pa.nchunks + 2 * pa.depth) * per_round;  // the host keeps this below 2^31
+    auto prefetch_a = [&](uint32_t it, uint4* buf) {  // the rows of a pass-A item, if it is one
+        if (it >= total) return;
+        const PipeItem pi = pipe_decode(pa, it, per_round);
+        if (pi.ph == 0 && pi.c < (int64_t)pa.nchunks)
+            step_prefetch<PLA, SF_EXT_A>(buf, pipe_args<0>(pa, (uint32_t)pi.c), pi.j, tid % PLA::Q4, tid / PLA::Q4);
+    };
     if (tid == 0) {
         s_item = atomicAdd(pa.counters, 1u);
+        s_next[0] = atomicAdd(pa.counters, 1u);
         s_fail = 0;
     }
     __syncthreads();
-    uint32_t item = s_item;
-    while (item < total) {
-        __syncthreads();  // every thread has read s_item
-        uint32_t nxt = 0;
-        if (tid == 0) nxt = atomicAdd(pa.counters, 1u);  // drawn now, used after the tile
-        const uint32_t r = item / per_round;
-        uint32_t j = item - r * per_round;
-        int ph = 0;
-        int64_t c = r;
-        if (j >= pa.tiles[0]) {
-            j -= pa.tiles[0];
-            if (j < pa.tiles[1]) {
-                ph = 1;
-                c = (int64_t)r - pa.depth;
-            } else {
-                j -= pa.tiles[1];
-                ph = 2;
-                c = (int64_t)r - 2 * (int64_t)pa.depth;
-            }
+    uint32_t item = s_item, next = s_next[0];
+    int b = 0;
+    if constexpr (STAGE) {
+        prefetch_a(item, sm);
+        cp_async_commit();
+    }
+    // Every item ends with one barrier: the item's tile is stored (and, before a
+    // pass-A or block tile is counted, fenced by thread 0: the fence is cumulative
+    // over the stores the barrier ordered before it), its shared memory reads are
+    // done, and s_next is published. The next item's first shared-memory write,
+    // or a copy into the other buffer, comes after that barrier.
+    for (uint32_t it = 0; item < total; it++) {
+        uint32_t nn = 0;
+        if (tid == 0) nn = atomicAdd(pa.counters, 1u);  // the item after next, used after this tile
+        uint4* buf = sm;
+        if constexpr (STAGE) {
+            buf = sm + b * BUF;
+            prefetch_a(next, sm + (b ^ 1) * BUF);
+            cp_async_commit();
         }
-        if (c >= 0 && c < (int64_t)pa.nchunks) {
-            const uint32_t cc = (uint32_t)c;
-            if (ph > 0) {
+        const PipeItem pi = pipe_decode(pa, item, per_round);
+        if (pi.c >= 0 && pi.c < (int64_t)pa.nchunks) {
+            const uint32_t cc = (uint32_t)pi.c;
+            if (pi.ph > 0) {
                 if (tid == 0) {
-                    const uint32_t* done = pa.counters + 1 + (ph == 1 ? 0u : pa.nchunks) + cc;
-                    if (!pipe_wait_count(done, pa.tiles[ph - 1])) {
+                    const uint32_t* done = pa.counters + 1 + (pi.ph == 1 ? 0u : pa.nchunks) + cc;
+                    if (!pipe_wait_count(done, pa.tiles[pi.ph - 1])) {
                         s_fail = 1;
                         atomicOr(pa.err, 4);
                     }
                     __threadfence();
                 }
                 __syncthreads();
-                if (s_fail) return;
+                if (s_fail) {
+                    if constexpr (STAGE) cp_async_wait<0>();
+                    return;
+                }
             }
-            if (ph == 0) pipe_pass<0, L1, L2, SHAPE>(pa, cc, j, sm, tid, tw, tw_lo);
-            else if (ph == 1) pipe_pass<1, L1, L2, SHAPE>(pa, cc, j, sm, tid, tw, tw_lo);
-            else pipe_pass<2, L1, L2, SHAPE>(pa, cc, j, sm, tid, tw, tw_lo);
-            if (ph < 2) {
-                __threadfence();  // this thread's stores of the tile, before the count
-                __syncthreads();
-                if (tid == 0) atomicAdd(pa.counters + 1 + (ph == 0 ? 0u : pa.nchunks) + cc, 1u);
+            if (pi.ph == 0) {
+                if constexpr (STAGE) cp_async_wait<1>();  // this item's rows (the newest group is the next item's)
+                pipe_pass<0, L1, L2, SHAPE, STAGE>(pa, cc, pi.j, buf, tid, tw, tw_lo);
+            } else if (pi.ph == 1) {
+                pipe_pass<1, L1, L2, SHAPE, STAGE>(pa, cc, pi.j, buf, tid, tw, tw_lo);
+            } else {
+                pipe_pass<2, L1, L2, SHAPE, STAGE>(pa, cc, pi.j, buf, tid, tw, tw_lo);
             }
         }
-        if (tid == 0) s_item = nxt;
+        if (tid == 0) s_next[(it + 1) & 1] = nn;
         __syncthreads();
-        item = s_item;
+        if (tid == 0 && pi.ph < 2 && pi.c >= 0 && pi.c < (int64_t)pa.nchunks) {
+            __threadfence();  // every thread's stores of the tile (ordered by the barrier), before the count
+            atomicAdd(pa.counters + 1 + (pi.ph == 0 ? 0u : pa.nchunks) + (uint32_t)pi.c, 1u);
+        }
+        item = next;
+        next = s_next[(it + 1) & 1];
+        b ^= 1;
     }
+    if constexpr (STAGE) cp_async_wait<0>();
 }
 
 }  // namespace zb
