@@ -86,6 +86,11 @@ enum : int {
     // (tw_at_c) passed in place of the omega_8192 table, takes its output twiddle
     // as post-factors (no SF_TW), mid1 alone (mid2 unused), and no SF_CNT.
     SF_FOLD = 1024,
+    // SF_NOPREBAR: the caller has already ordered the previous tile's last reads of
+    // shared memory before this tile (the pipelined launch's per-item barrier), so
+    // the first exchange write needs no barrier of its own (direct loads only: a
+    // staged tile's buffer is still being read by other threads)
+    SF_NOPREBAR = 2048,
     // the extension's passes (long_extend): strided INTT with its output twiddle
     // (a post-factor table) and the even-row copy; block pass with the middle
     // factor and its output twiddle; strided NTT
@@ -316,7 +321,7 @@ struct FacTw {
 // Levels l .. NLEV-2 of one transform, each level's twiddles folded into its last
 // butterfly stage; returns with the last level's input in v. The write of level 0
 // waits for the previous tile's last exchange reads.
-template <class PL, int l, bool INV, bool MIR>
+template <class PL, int l, bool INV, bool MIR, bool PREBAR = true>
 __device__ __forceinline__ void fs_levels(V4* v, uint4* sm, int t, int q, const Tw* twc) {
     using LV = LvlOf<PL, l, MIR>;
     if constexpr (l > 0) LV::read(v, sm, t, q);
@@ -324,7 +329,7 @@ __device__ __forceinline__ void fs_levels(V4* v, uint4* sm, int t, int q, const 
 #pragma unroll
         for (int g = 0; g < LV::G; g++)
             dft_dif_twout<LV::LRADIX, INV, true>(v + g * LV::R, LvlTw<INV, LV::LOGN>{twc, LV::n1(LV::gid(g, t))});
-        if constexpr (l == 0) __syncthreads();
+        if constexpr (l == 0 && PREBAR) __syncthreads();
         LV::write(v, sm, t, q);
         __syncthreads();
         fs_levels<PL, l + 1, INV, MIR>(v, sm, t, q, twc);
@@ -367,7 +372,8 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, uint64_t tile, uint
     if constexpr (STAGED) step_consume<PL, F>(v, sm, a, p, q, t);
     else step_load<PL, LD_L2, F>(v, a, p, t);
     if constexpr (F & SF_FOLD) {
-        fs_levels<PL, 0, INV, false>(v, sm, t, q, tw);  // tw: the compact table
+        static_assert(!(STAGED && (F & SF_NOPREBAR)), "a staged tile's buffer needs the barrier");
+        fs_levels<PL, 0, INV, false, !(F & SF_NOPREBAR)>(v, sm, t, q, tw);  // tw: the compact table
         fs_last_store<PL, INV, false, ST_KEEP, F>(v, t, a, p);
         return;
     }
@@ -440,7 +446,8 @@ __device__ __forceinline__ void step2_tile(const StepArgs& a, uint64_t tile, uin
     if constexpr (F & SF_FOLD) {
         static_assert(!(F & SF_CNT), "the count reads T1's outputs before the middle factor");
         static_assert(PL::NLEV > 1, "T2 exchanges after its first level");
-        fs_levels<PL, 0, INV1, false>(v, sm, t, q, tw);
+        static_assert(!(STAGED && (F & SF_NOPREBAR)), "a staged tile's buffer needs the barrier");
+        fs_levels<PL, 0, INV1, false, !(F & SF_NOPREBAR)>(v, sm, t, q, tw);
         constexpr int LR = PL::lr(PL::NLEV - 1);
         constexpr int R = 1 << LR;
         constexpr int G = PL::EPT / R;
@@ -645,12 +652,14 @@ __device__ __forceinline__ void pipe_pass(const PipeArgs& pa, uint32_t c, uint32
                                           const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo) {
     const StepArgs x = pipe_args<PH>(pa, c);
     if constexpr (PH == 0) {
-        step_tile<L1, true, SHAPE, false, true, STAGED0, SF_EXT_A>(x, tile, sm, tid, tw, tw_lo);
+        step_tile<L1, true, SHAPE, false, true, STAGED0, STAGED0 ? SF_EXT_A : (SF_EXT_A | SF_NOPREBAR)>(
+            x, tile, sm, tid, tw, tw_lo);
     } else if constexpr (PH == 1) {
         unsigned long long cnt = 0;
-        step2_tile<L2, true, false, SHAPE, true, true, false, SF_EXT_M>(x, tile, sm, tid, tw, tw_lo, cnt);
+        step2_tile<L2, true, false, SHAPE, true, true, false, SF_EXT_M | SF_NOPREBAR>(x, tile, sm, tid, tw, tw_lo,
+                                                                                    cnt);
     } else {
-        step_tile<L1, false, SHAPE, true, false, false, SF_EXT_B>(x, tile, sm, tid, tw, tw_lo);
+        step_tile<L1, false, SHAPE, true, false, false, SF_EXT_B | SF_NOPREBAR>(x, tile, sm, tid, tw, tw_lo);
     }
 }
 
