@@ -143,16 +143,16 @@ def model_extend(data: np.ndarray) -> np.ndarray:
     return out.reshape(2 * S, cols).astype(np.uint32)
 
 
-def pipe_geometry(L: int, q4a: int, q4m: int, grid: int, cols: int) -> dict:
-    """fourstep.cu pipe_t: chunk quads, tiles per chunk and pass, chunks, depth."""
+def pipe_geometry(L: int, q4a: int, q4m: int, grid: int, cols: int, tpi: int = 1) -> dict:
+    """fourstep.cu pipe_t: chunk quads, work items (of tpi tiles) per chunk and pass, chunks, depth."""
     L1, L2, N1, N2 = split(L)
     cq = max(q4a, q4m)
     quads = cols // 4
     nch = -(-quads // cq)
-    tiles = [N2 * cq // q4a, N1 * cq // q4m, N2 * cq // q4a]
+    tiles = [N2 * cq // q4a // tpi, N1 * cq // q4m // tpi, N2 * cq // q4a // tpi]
     per_round = sum(tiles)
     depth = max(1, -(-(2 * 3 * grid) // per_round))
-    return dict(cq=cq, nch=nch, tiles=tiles, per_round=per_round, depth=depth,
+    return dict(cq=cq, nch=nch, tiles=tiles, per_round=per_round, depth=depth, tpi=tpi,
                 last_qlim=quads - (nch - 1) * cq, total=(nch + 2 * depth) * per_round)
 
 
@@ -169,7 +169,7 @@ def pipe_decode(item: int, g: dict):
     return ph, (c if 0 <= c < g["nch"] else None), j
 
 
-def model_extend_pipelined(data: np.ndarray, q4a: int, q4m: int, grid: int, seed: int) -> np.ndarray:
+def model_extend_pipelined(data: np.ndarray, q4a: int, q4m: int, grid: int, seed: int, tpi: int = 1) -> np.ndarray:
     """k_fourstep_pipe: the passes of long_extend as tiles of (chunk, pass), dealt in the
     kernel's order to `grid` CTAs that each hold one item and the two drawn after it, and
     finished in a random order among those whose dependencies are met (a pass-B or block
@@ -178,7 +178,7 @@ def model_extend_pipelined(data: np.ndarray, q4a: int, q4m: int, grid: int, seed
     S, cols = data.shape
     L = S.bit_length() - 1
     L1, L2, N1, N2 = split(L)
-    g = pipe_geometry(L, q4a, q4m, grid, cols)
+    g = pipe_geometry(L, q4a, q4m, grid, cols, tpi)
     cq = g["cq"]
     inp = data.astype(np.uint64).ravel()
     out = np.full(2 * S * cols, 12345, dtype=np.uint64)
@@ -230,9 +230,11 @@ def model_extend_pipelined(data: np.ndarray, q4a: int, q4m: int, grid: int, seed
         if c is not None:
             assert (ph, c, j) not in ran
             ran.add((ph, c, j))
-            a, q4 = args(ph, c)
-            a["quads"] = (j * q4, j * q4 + q4)
-            model_pass(a)
+            for u in range(tpi):  # the item's tiles in turn
+                a, q4 = args(ph, c)
+                t = j * tpi + u
+                a["quads"] = (t * q4, t * q4 + q4)
+                model_pass(a)
             if ph < 2:
                 done[ph][c] += 1
         ctas[k] = [nxt, after, draw()]
@@ -388,10 +390,12 @@ def test_model_recover():
 @pytest.mark.parametrize("L,q4a,q4m,grid,cols", [(10, 256, 256, 3, 4 * 256 * 3 + 8), (11, 256, 128, 5, 4 * 256 * 4 + 12),
                                                  (12, 128, 128, 7, 4 * 128 * 5 + 4), (12, 32, 32, 16, 4 * 32 * 9 + 20),
                                                  (13, 128, 64, 4, 4 * 128 * 3 + 16)])
-def test_model_pipelined_extension_matches_oracle(L, q4a, q4m, grid, cols):
+@pytest.mark.parametrize("tpi", [1, 2, 4])
+def test_model_pipelined_extension_matches_oracle(L, q4a, q4m, grid, cols, tpi):
     S = 1 << L
     data = O.seeded_input(S, cols, seed=L + cols)
-    assert np.array_equal(model_extend_pipelined(data, q4a, q4m, grid, seed=L), O.encode_rowmajor(data))
+    assert np.array_equal(model_extend_pipelined(data, q4a, q4m, grid, seed=L + tpi, tpi=tpi),
+                          O.encode_rowmajor(data))
 
 
 def test_pipe_geometry_limits():

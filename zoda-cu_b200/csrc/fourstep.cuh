@@ -615,7 +615,8 @@ struct PipeArgs {
     uint64_t chunk_u32;  // u32 from one chunk's first column to the next chunk's
     uint32_t nchunks;
     uint32_t last_qlim;  // real quads in the last chunk
-    uint32_t tiles[3];   // tiles per chunk of each pass
+    uint32_t tiles[3];   // work items per chunk of each pass
+    uint32_t tpi;        // tiles per work item (1 in the staged form)
     uint32_t depth;      // rounds between a chunk's passes
     uint32_t* counters;  // [0] item counter; [1 + c] pass-A tiles done; [1 + nchunks + c] block tiles done
     int* err;
@@ -758,13 +759,19 @@ __global__ void __launch_bounds__(PipeShape<L1, L2, SHAPE>::THREADS,
                     return;
                 }
             }
-            if (pi.ph == 0) {
-                if constexpr (STAGE) cp_async_wait<1>();  // this item's rows (the newest group is the next item's)
-                pipe_pass<0, L1, L2, SHAPE, STAGE>(pa, cc, pi.j, buf, tid, tw, tw_lo);
-            } else if (pi.ph == 1) {
-                pipe_pass<1, L1, L2, SHAPE, STAGE>(pa, cc, pi.j, buf, tid, tw, tw_lo);
-            } else {
-                pipe_pass<2, L1, L2, SHAPE, STAGE>(pa, cc, pi.j, buf, tid, tw, tw_lo);
+            // the item's tiles in turn; a barrier between two of them orders the first
+            // one's last exchange reads before the next one's first exchange write
+            for (uint32_t u = 0; u < pa.tpi; u++) {
+                const uint32_t tile = pi.j * pa.tpi + u;
+                if (u) __syncthreads();
+                if (pi.ph == 0) {
+                    if constexpr (STAGE) cp_async_wait<1>();  // this item's rows (the newest group is the next item's)
+                    pipe_pass<0, L1, L2, SHAPE, STAGE>(pa, cc, tile, buf, tid, tw, tw_lo);
+                } else if (pi.ph == 1) {
+                    pipe_pass<1, L1, L2, SHAPE, STAGE>(pa, cc, tile, buf, tid, tw, tw_lo);
+                } else {
+                    pipe_pass<2, L1, L2, SHAPE, STAGE>(pa, cc, tile, buf, tid, tw, tw_lo);
+                }
             }
         }
         if (tid == 0) s_next[(it + 1) & 1] = nn;
