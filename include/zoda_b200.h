@@ -202,11 +202,19 @@ zoda_status zoda_extend_host(zoda_ctx* ctx, const uint32_t* h_in, uint32_t* h_ou
 
 /* Fault injection for tests of the error paths; no counterpart in the
  * reference. Arms `site`: the call passes through it `after` more times, then
- * the next pass fails with ZODA_ERR_CUDA (zoda_last_error says "injected
- * fault") and the site disarms. site 0 disarms everything. Sites:
+ * the next pass fails and the site disarms. site 0 disarms everything. Sites:
  *   ZODA_FAULT_HOST_CHUNK  the launch of one column chunk in zoda_extend_host,
- *                          after earlier chunks' copies have been queued. */
+ *                          after earlier chunks' copies have been queued: the
+ *                          call fails with ZODA_ERR_CUDA (zoda_last_error says
+ *                          "injected fault");
+ *   ZODA_FAULT_PIPE_WAIT   one pipelined four-step launch (plan impl 3,
+ *                          blocked 1) waits for one finished tile more than a
+ *                          chunk has: its bounded dependency waits run out
+ *                          (about a second), every CTA flags the error and
+ *                          leaves, and zoda_ctx_check reports ZODA_ERR_TIMEOUT
+ *                          (the output is then incomplete). */
 #define ZODA_FAULT_HOST_CHUNK 1u
+#define ZODA_FAULT_PIPE_WAIT 2u
 zoda_status zoda_ctx_inject_fault(zoda_ctx* ctx, uint32_t site, uint32_t after);
 
 /* ----------------------------------------------------------------------

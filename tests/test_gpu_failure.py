@@ -63,3 +63,41 @@ def test_host_call_error_returns_with_no_copy_outstanding():
         assert t.h2d_bytes == side * cols * 4 and t.d2h_bytes >= side * cols * 4
     finally:
         c.close()
+
+
+def test_pipelined_fourstep_wait_runs_out_and_the_context_survives():
+    """The pipelined four-step launch (one persistent launch whose block-pass and
+    pass-B tiles wait on per-chunk counts of finished tiles) is told to wait for one
+    tile more than a chunk has (ZODA_FAULT_PIPE_WAIT): every wait runs out after
+    about a second, each CTA flags the error and leaves, the context reports
+    ZODA_ERR_TIMEOUT once, and the next launch is bit-exact again. No GPU fault:
+    the waits are bounded polls of a counter in device memory."""
+    import time
+
+    import zoda_b200
+    c = zoda_b200.Context(0)
+    side, cols = 1024, 4096
+    try:
+        c.plan_set(side, {"impl": 3, "sched": 0, "l2_promo": 3, "blocked": 1, "stagger": 1, "radix": 8,
+                          "ctas": 4})
+        data = O.seeded_input(side, cols, seed=17)
+        d_in = torch.from_numpy(data.view(np.int32)).cuda()
+        d_out = torch.empty((2 * side, cols), dtype=torch.int32, device="cuda")
+        c.check()
+        c.inject_fault(2)
+        t0 = time.perf_counter()
+        c.extend(d_in, d_out, side, cols)
+        torch.cuda.synchronize()
+        elapsed = time.perf_counter() - t0
+        with pytest.raises(zoda_b200.ZodaError) as e:
+            c.check()
+        assert e.value.status == ZODA_ERR_TIMEOUT
+        assert elapsed < 30.0  # bounded: about a second of polling per CTA, the CTAs in parallel
+        c.check()  # the flag was cleared
+        c.extend(d_in, d_out, side, cols)  # the fault disarmed itself
+        torch.cuda.synchronize()
+        c.check()
+        assert np.array_equal(d_out.cpu().numpy().view(np.uint32), O.encode_rowmajor(data))
+    finally:
+        c.plan_clear()
+        c.close()

@@ -358,7 +358,7 @@ zoda_status zoda_extend_device(zoda_ctx* ctx, const uint32_t* d_in, uint32_t* d_
 }
 
 zoda_status zoda_ctx_inject_fault(zoda_ctx* ctx, uint32_t site, uint32_t after) {
-    if (!ctx || site > ZODA_FAULT_HOST_CHUNK) return ZODA_ERR_ARG;
+    if (!ctx || site > ZODA_FAULT_PIPE_WAIT) return ZODA_ERR_ARG;
     std::lock_guard<std::mutex> lock(ctx->mu);
     ctx->fault_site = site;
     ctx->fault_after = after;

@@ -303,6 +303,10 @@ zoda_status pipe_t(const zoda_ctx* ctx, const StepArgs pass[3], uint64_t cols, c
     if (!mc->pipe_done) ZB_CUDA(cudaEventCreateWithFlags(&mc->pipe_done, cudaEventDisableTiming));
     pa.counters = (uint32_t*)mc->pipe_cnt.p;
     pa.err = ctx->d_err;
+    if (mc->fault_site == ZODA_FAULT_PIPE_WAIT && mc->fault_after-- == 0) {
+        mc->fault_site = 0;
+        pa.wait_extra = 1;  // a count no chunk reaches: every dependency wait runs out
+    }
     // launches on other streams share the counters: each waits for the one before
     ZB_CUDA(cudaStreamWaitEvent(st, mc->pipe_done, 0));
     ZB_CUDA(cudaMemsetAsync(pa.counters, 0, cbytes, st));

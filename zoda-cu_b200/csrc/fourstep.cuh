@@ -617,6 +617,7 @@ struct PipeArgs {
     uint32_t last_qlim;  // real quads in the last chunk
     uint32_t tiles[3];   // work items per chunk of each pass
     uint32_t tpi;        // tiles per work item (1 in the staged form)
+    uint32_t wait_extra; // added to every dependency count a work item waits for (fault injection: 1)
     uint32_t depth;      // rounds between a chunk's passes
     uint32_t* counters;  // [0] item counter; [1 + c] pass-A tiles done; [1 + nchunks + c] block tiles done
     int* err;
@@ -747,7 +748,7 @@ __global__ void __launch_bounds__(PipeShape<L1, L2, SHAPE>::THREADS,
             if (pi.ph > 0) {
                 if (tid == 0) {
                     const uint32_t* done = pa.counters + 1 + (pi.ph == 1 ? 0u : pa.nchunks) + cc;
-                    if (!pipe_wait_count(done, pa.tiles[pi.ph - 1])) {
+                    if (!pipe_wait_count(done, pa.tiles[pi.ph - 1] + pa.wait_extra)) {
                         s_fail = 1;
                         atomicOr(pa.err, 4);
                     }

@@ -334,7 +334,8 @@ class Context:
 
     def inject_fault(self, site: int, after: int = 0):
         """Arm a fault site (zoda_ctx_inject_fault): 1 = a column-chunk launch of
-        extend_host, failing after `after` chunks; 0 disarms."""
+        extend_host, failing after `after` chunks; 2 = a pipelined four-step launch
+        whose dependency waits run out; 0 disarms."""
         _check(load().zoda_ctx_inject_fault(self._h, site, after), "zoda_ctx_inject_fault")
 
     def extend_host(self, h_in, h_out, k: int, cols: int) -> ZodaTiming:
