@@ -128,8 +128,9 @@ typedef struct zoda_plan {
                          from k = 64)                                              */
     float ms;         /* the tuner's time for this plan (0 when set by hand)            */
     int32_t ctas;     /* FOURSTEP: CTAs resident per SM in its passes, 1 (512 threads),
-                         2 (256 threads at radix 16, 512 at radix 8) or 4 (256 threads,
-                         radix 8); 0 counts as 1. Ignored by the other kernels.    */
+                         2 (256 threads at radix 16, 512 at radix 8), 4 (256 threads,
+                         radix 8) or 5 (256 threads, radix 4: the one plan that takes
+                         radix 4); 0 counts as 1. Ignored by the other kernels.     */
 } zoda_plan;
 
 /* Times every candidate plan for each power-of-two side in [side_min,

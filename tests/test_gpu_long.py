@@ -128,7 +128,7 @@ def test_long_extension_matches_oracle(ctx, side, cols):
     assert np.array_equal(from_dev(d_out), O.encode_rowmajor(data))
 
 
-FOURSTEP_SHAPES = [(16, 1), (16, 2), (8, 2), (8, 4)]
+FOURSTEP_SHAPES = [(16, 1), (16, 2), (8, 2), (8, 4), (4, 5)]
 
 
 # plan forms: (sched, blocked) = three launches, three staged launches (cp.async

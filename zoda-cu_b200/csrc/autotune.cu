@@ -96,7 +96,7 @@ std::vector<zoda_plan> candidates(int ls) {
     // (blocked 0) or one launch that runs them column chunk by column chunk
     // (blocked 1), each with or without tiles staged by cp.async (sched 1)
     for (int form = 0; form < 4 && ls >= FOURSTEP_MIN_LOG; form++)
-        for (const auto& rc : {std::pair<int, int>{16, 1}, {16, 2}, {8, 2}, {8, 4}}) {
+        for (const auto& rc : {std::pair<int, int>{16, 1}, {16, 2}, {8, 2}, {8, 4}, {4, 5}}) {
             if ((form & 1) && rc.second == 1) continue;
             const int blocked = form >= 2;
             zoda_plan p = d;

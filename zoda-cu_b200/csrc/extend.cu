@@ -127,14 +127,16 @@ zoda_status check_plan(int log_s, const zoda_plan& p) {
     if (p.impl == ZODA_IMPL_TMA && log_s < 5) return ZODA_ERR_UNSUPPORTED;
     if (p.impl == ZODA_IMPL_FOURSTEP) {
         if (log_s < FOURSTEP_MIN_LOG) return ZODA_ERR_UNSUPPORTED;
-        if (p.ctas < 0 || p.ctas > 4 || p.ctas == 3 || (p.radix == 16 && p.ctas == 4) ||
-            (p.radix == 8 && p.ctas <= 1))
-            return ZODA_ERR_ARG;
+        // (radix, CTAs per SM): (16, 1), (16, 2), (8, 2), (8, 4), (4, 5); ctas 0 counts as 1
+        const int c = p.ctas == 0 ? 1 : p.ctas;
+        const bool shape_ok = (p.radix == 16 && (c == 1 || c == 2)) || (p.radix == 8 && (c == 2 || c == 4)) ||
+                              (p.radix == 4 && c == 5);
+        if (!shape_ok) return ZODA_ERR_ARG;
         // sched 1: staged passes, which exist for the shapes of 2 and 4 CTAs per SM
         if (p.sched == 1 && p.ctas <= 1) return ZODA_ERR_ARG;
     }
     if (p.sched < 0 || p.sched > 1 || p.l2_promo < 0 || p.l2_promo > 3 || p.blocked < 0 || p.blocked > 1 ||
-        p.stagger < 0 || p.stagger > 3 || (p.radix != 16 && p.radix != 8))
+        p.stagger < 0 || p.stagger > 3 || (p.radix != 16 && p.radix != 8 && !(p.radix == 4 && p.impl == ZODA_IMPL_FOURSTEP)))
         return ZODA_ERR_ARG;
     if (p.radix == 8 && p.impl == ZODA_IMPL_DIRECT && log_s < 6) return ZODA_ERR_UNSUPPORTED;
     return ZODA_OK;

@@ -127,6 +127,7 @@ zoda_status ext_pass_shape(const zoda_ctx* ctx, int shape, const StepArgs& a, cu
         case 1: return ext_pass_t<LOG_N, PASS, 1>(ctx, staged, a, st);
         case 2: return ext_pass_t<LOG_N, PASS, 2>(ctx, staged, a, st);
         case 3: return ext_pass_t<LOG_N, PASS, 3>(ctx, staged, a, st);
+        case 4: return ext_pass_t<LOG_N, PASS, 4>(ctx, staged, a, st);
         default: return ext_pass_t<LOG_N, PASS, 0>(ctx, staged, a, st);
     }
 }
@@ -326,6 +327,7 @@ zoda_status pipe_shape(const zoda_ctx* ctx, int shape, const StepArgs pass[3], u
         case 1: return staged ? pipe_t<L1, L2, 1, true>(ctx, pass, cols, st) : pipe_t<L1, L2, 1, false>(ctx, pass, cols, st);
         case 2: return staged ? pipe_t<L1, L2, 2, true>(ctx, pass, cols, st) : pipe_t<L1, L2, 2, false>(ctx, pass, cols, st);
         case 3: return staged ? pipe_t<L1, L2, 3, true>(ctx, pass, cols, st) : pipe_t<L1, L2, 3, false>(ctx, pass, cols, st);
+        case 4: return staged ? pipe_t<L1, L2, 4, true>(ctx, pass, cols, st) : pipe_t<L1, L2, 4, false>(ctx, pass, cols, st);
         default: return staged ? ZODA_ERR_UNSUPPORTED : pipe_t<L1, L2, 0, false>(ctx, pass, cols, st);
     }
 }
@@ -337,7 +339,7 @@ zoda_status pipe_shape(const zoda_ctx* ctx, int shape, const StepArgs pass[3], u
 // coset_mid_tables(ctx, L, L + 1).
 int fourstep_shape(int radix, int ctas, bool staged) {
     if (ctas <= 1) return 0;
-    const int shape = radix == 16 ? 1 : ctas == 2 ? 2 : 3;
+    const int shape = radix == 16 ? 1 : radix == 4 ? 4 : ctas == 2 ? 2 : 3;
     return shape | (staged ? STEP_STAGED : 0);
 }
 

@@ -264,14 +264,13 @@ __device__ __forceinline__ void step_consume(V4* v, const uint4* stage, const St
 // which the single-CTA shape cannot do: its loads go straight to registers).
 //   0: radix 16 / 512 threads (radix 8 / 1024 from 512 points), one CTA per SM
 //   1: radix 16, 256 threads, 2 per SM      2: radix 8, 512 threads, 2 per SM
-//   3: radix 8, 256 threads, 4 per SM       (1..3: transforms of 32..256 points)
-constexpr int STEP_SHAPES = 4;
-constexpr int STEP_SHAPE_MAX_LOG = 8;
+//   3: radix 8, 256 threads, 4 per SM       4: radix 4, 256 threads, 5 per SM
+//   (1..4: the extension's passes, 32..128 points)
 template <int LOG_N, int SHAPE>
 struct StepShape {
-    static constexpr int LEPT = SHAPE == 0 ? (LOG_N >= 9 ? 3 : 4) : SHAPE == 1 ? 4 : 3;
+    static constexpr int LEPT = SHAPE == 0 ? (LOG_N >= 9 ? 3 : 4) : SHAPE == 1 ? 4 : SHAPE == 4 ? 2 : 3;
     static constexpr int THREADS = SHAPE == 0 ? (LOG_N >= 9 ? 1024 : 512) : SHAPE == 2 ? 512 : 256;
-    static constexpr int MINB = SHAPE == 0 ? 1 : SHAPE == 3 ? 4 : 2;
+    static constexpr int MINB = SHAPE == 0 ? 1 : SHAPE == 3 ? 4 : SHAPE == 4 ? 5 : 2;
     using PL = ExtPlan<LOG_N, 0, LEPT, THREADS>;
     // staged passes hold two tiles (the next one arriving, the current one, which
     // also serves as the exchange buffer): CTAs per SM that fit 227 KB

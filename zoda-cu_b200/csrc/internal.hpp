@@ -170,7 +170,7 @@ zoda_status long_extend(const zoda_ctx* ctx, int L, const uint2* tabs, const uin
                         bool pipelined = false);
 // The four-step launch shape of a plan's (radix, ctas); staged adds STEP_STAGED (the
 // passes copy each next tile in by cp.async while the current one computes).
-constexpr int STEP_STAGED = 4;
+constexpr int STEP_STAGED = 8;
 int fourstep_shape(int radix, int ctas, bool staged = false);
 // Smallest side (log2) the four-step plan covers.
 constexpr int FOURSTEP_MIN_LOG = 10;
