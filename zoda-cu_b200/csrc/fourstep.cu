@@ -246,13 +246,18 @@ zoda_status long_cols_ntt(const zoda_ctx* ctx, uint32_t* B, uint32_t* A, int L, 
 
 // The same three passes in one persistent launch, column chunk by column chunk
 // (k_fourstep_pipe), so each chunk's intermediate stays in L2 between its passes.
-// The most tiles one work item of the pipelined launch covers (measured at side
-// 4096, CUDA events: 12.96 ms with 1, 12.82 with 4, 12.72 with 8).
+// The most tiles one work item of the pipelined launch covers, and the pipeline
+// depth in units of the items the CTAs hold (measured at side 4096, CUDA events,
+// on one box each: 1 tile and depth 2 12.96 ms, 4 and 2 12.82, 8 and 2 12.72-12.82,
+// 8 and 1 12.96-13.03, 1 and 1 13.05, 2 and 1 12.71).
 #ifndef ZB_PIPE_TILES
-#define ZB_PIPE_TILES 8
+#define ZB_PIPE_TILES 2
 #endif
 static_assert(ZB_PIPE_TILES >= 1 && ZB_PIPE_TILES <= 32 && (ZB_PIPE_TILES & (ZB_PIPE_TILES - 1)) == 0,
               "tiles per work item: a power of two that divides every pass's tile count");
+#ifndef ZB_PIPE_DEPTH_HELD
+#define ZB_PIPE_DEPTH_HELD 1
+#endif
 
 template <int L1, int L2, int SHAPE, bool STAGE>
 zoda_status pipe_t(const zoda_ctx* ctx, const StepArgs pass[3], uint64_t cols, cudaStream_t st) {
@@ -289,10 +294,12 @@ zoda_status pipe_t(const zoda_ctx* ctx, const StepArgs pass[3], uint64_t cols, c
     constexpr size_t smem = (STAGE ? 2 : 1) * PS::SMEM;
     const uint64_t grid = (uint64_t)ctx->sm_count * minb;
     const uint64_t per_round = (uint64_t)pa.tiles[0] + pa.tiles[1] + pa.tiles[2];
-    // depth: enough rounds between a chunk's passes that its earlier tiles are done
-    // before the later ones are dealt (twice the items the CTAs hold at once: the
-    // current one and the two drawn ahead)
-    uint64_t depth = (2 * 3 * grid + per_round - 1) / per_round;
+    // depth: enough rounds between a chunk's passes that its earlier tiles are
+    // mostly done before the later ones are dealt, measured in the items the CTAs
+    // hold at once (the current one and the two drawn ahead): ZB_PIPE_DEPTH_HELD
+    // times that many items. A deeper pipeline waits less but keeps more chunks'
+    // intermediates in flight, and those stay in L2 only while they fit.
+    uint64_t depth = ((uint64_t)ZB_PIPE_DEPTH_HELD * 3 * grid + per_round - 1) / per_round;
     if (depth < 1) depth = 1;
     pa.depth = (uint32_t)depth;
     if (nch > (1u << 30) || (nch + 2 * depth) * per_round + 3 * grid >= (1ull << 31)) return ZODA_ERR_UNSUPPORTED;
