@@ -117,8 +117,8 @@ zoda_status ext_pass_t(const zoda_ctx* ctx, bool staged, const StepArgs& a, cuda
         if (staged) return step_st_t<LOG_N, INV, PASS == 1, SHAPE, F>(ctx, a, st);
     }
     if (staged) return ZODA_ERR_UNSUPPORTED;
-    if constexpr (PASS == 1) return step2_t<LOG_N, true, SHAPE, F>(ctx, a, st);
-    else return step_t<LOG_N, INV, SHAPE, F>(ctx, a, st);
+    if constexpr (PASS == 1) return step2_t<LOG_N, true, SHAPE, F | SF_PASS_GROUPS>(ctx, a, st);
+    else return step_t<LOG_N, INV, SHAPE, F | SF_PASS_GROUPS>(ctx, a, st);
 }
 template <int LOG_N, int PASS>
 zoda_status ext_pass_shape(const zoda_ctx* ctx, int shape, const StepArgs& a, cudaStream_t st) {

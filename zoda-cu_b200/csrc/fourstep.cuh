@@ -23,6 +23,7 @@
 //   * k_step2<.., false, true>: pass B of an NTT, the factor, pass A of the
 //     following INTT with the same decomposition: a "strided" pass.
 #pragma once
+#include "async.cuh"
 #include "extend.cuh"
 
 namespace zb {
@@ -67,6 +68,12 @@ struct StepArgs {
     unsigned long long* counter;  // or nullptr
 };
 
+// Whether the extension's folded passes that load straight from memory split the
+// CTA into two barrier groups (SF_GROUPS).
+#ifndef ZB_PASS_GROUPS
+#define ZB_PASS_GROUPS 1
+#endif
+
 // Features a pass may use, as compile-time flags: a pass instantiated without a
 // flag drops that feature's code and its runtime test (SF_ALL keeps every test).
 enum : int {
@@ -91,6 +98,12 @@ enum : int {
     // the first exchange write needs no barrier of its own (direct loads only: a
     // staged tile's buffer is still being read by other threads)
     SF_NOPREBAR = 2048,
+    // SF_GROUPS (with SF_FOLD, loads straight from memory): the CTA's threads form
+    // two halves, each owning half of the tile's column quads and their exchange
+    // slots, with its own named barrier, so one half's exchange waits do not hold
+    // the other half
+    SF_GROUPS = 4096,
+    SF_PASS_GROUPS = ZB_PASS_GROUPS ? SF_GROUPS : 0,  // the extension's direct-load passes
     // the extension's passes (long_extend): strided INTT with its output twiddle
     // (a post-factor table) and the even-row copy; block pass with the middle
     // factor and its output twiddle; strided NTT
@@ -317,21 +330,46 @@ struct FacTw {
     }
 };
 
+// A thread's quad q (of the tile's Q4) and row group t; with SF_GROUPS, half g of
+// the CTA (threads g*T/2 .. ) owns quads g*Q4/2 .. (g+1)*Q4/2 - 1, each half a
+// whole number of warps.
+template <class PL, int F>
+struct PassThread {
+    static constexpr bool GROUPS = (F & SF_GROUPS) != 0;
+    static constexpr int GS = GROUPS ? PL::THREADS / 2 : PL::THREADS;  // threads of a barrier group
+    static constexpr int GQ = GROUPS ? PL::Q4 / 2 : PL::Q4;            // quads of a group
+    static_assert(!GROUPS || (GS % 32 == 0 && GQ >= 1 && GS % GQ == 0), "halves of whole warps and quads");
+    int q, t, grp;
+    __device__ __forceinline__ explicit PassThread(int tid) {
+        grp = GROUPS ? tid / GS : 0;
+        const int l = tid - grp * GS;
+        q = grp * GQ + l % GQ;
+        t = l / GQ;
+    }
+    // the barrier between exchange writes and reads: the group's named barrier
+    // (ids 1 and 2), or the whole CTA's
+    __device__ __forceinline__ void bar() const {
+        if constexpr (GROUPS) group_bar(1 + grp, GS);
+        else __syncthreads();
+    }
+};
+
 // Levels l .. NLEV-2 of one transform, each level's twiddles folded into its last
 // butterfly stage; returns with the last level's input in v. The write of level 0
 // waits for the previous tile's last exchange reads.
-template <class PL, int l, bool INV, bool MIR, bool PREBAR = true>
-__device__ __forceinline__ void fs_levels(V4* v, uint4* sm, int t, int q, const Tw* twc) {
+template <class PL, int l, bool INV, bool MIR, bool PREBAR = true, class PT>
+__device__ __forceinline__ void fs_levels(V4* v, uint4* sm, const PT& pt, const Tw* twc) {
     using LV = LvlOf<PL, l, MIR>;
-    if constexpr (l > 0) LV::read(v, sm, t, q);
+    if constexpr (l > 0) LV::read(v, sm, pt.t, pt.q);
     if constexpr (l < PL::NLEV - 1) {
 #pragma unroll
         for (int g = 0; g < LV::G; g++)
-            dft_dif_twout<LV::LRADIX, INV, true>(v + g * LV::R, LvlTw<INV, LV::LOGN>{twc, LV::n1(LV::gid(g, t))});
-        if constexpr (l == 0 && PREBAR) __syncthreads();
-        LV::write(v, sm, t, q);
-        __syncthreads();
-        fs_levels<PL, l + 1, INV, MIR>(v, sm, t, q, twc);
+            dft_dif_twout<LV::LRADIX, INV, true>(v + g * LV::R,
+                                                 LvlTw<INV, LV::LOGN>{twc, LV::n1(LV::gid(g, pt.t))});
+        if constexpr (l == 0 && PREBAR) pt.bar();
+        LV::write(v, sm, pt.t, pt.q);
+        pt.bar();
+        fs_levels<PL, l + 1, INV, MIR, true, PT>(v, sm, pt, twc);
     }
 }
 
@@ -364,15 +402,17 @@ template <int LOG_N, bool INV, int SHAPE, bool LD_L2 = false, bool ST_KEEP = fal
 __device__ __forceinline__ void step_tile(const StepArgs& a, uint64_t tile, uint4* sm, int tid,
                                           const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo) {
     using PL = typename StepShape<LOG_N, SHAPE>::PL;
-    const int q = tid % PL::Q4;
-    const int t = tid / PL::Q4;
+    static_assert(!(F & SF_GROUPS) || ((F & SF_FOLD) && !STAGED), "groups: folded passes loading from memory");
+    const PassThread<PL, F> pt(tid);
+    const int q = pt.q;
+    const int t = pt.t;
     V4 v[PL::EPT];
     const QuadPos p(tile * PL::Q4 + q, a);
     if constexpr (STAGED) step_consume<PL, F>(v, sm, a, p, q, t);
     else step_load<PL, LD_L2, F>(v, a, p, t);
     if constexpr (F & SF_FOLD) {
         static_assert(!(STAGED && (F & SF_NOPREBAR)), "a staged tile's buffer needs the barrier");
-        fs_levels<PL, 0, INV, false, !(F & SF_NOPREBAR)>(v, sm, t, q, tw);  // tw: the compact table
+        fs_levels<PL, 0, INV, false, !(F & SF_NOPREBAR)>(v, sm, pt, tw);  // tw: the compact table
         fs_last_store<PL, INV, false, ST_KEEP, F>(v, t, a, p);
         return;
     }
@@ -436,8 +476,10 @@ __device__ __forceinline__ void step2_tile(const StepArgs& a, uint64_t tile, uin
                                            const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo,
                                            unsigned long long& cnt) {
     using PL = typename StepShape<LOG_N, SHAPE>::PL;
-    const int q = tid % PL::Q4;
-    const int t = tid / PL::Q4;
+    static_assert(!(F & SF_GROUPS) || ((F & SF_FOLD) && !STAGED), "groups: folded passes loading from memory");
+    const PassThread<PL, F> pt(tid);
+    const int q = pt.q;
+    const int t = pt.t;
     V4 v[PL::EPT];
     const QuadPos p(tile * PL::Q4 + q, a);
     if constexpr (STAGED) step_consume<PL, F>(v, sm, a, p, q, t);
@@ -446,7 +488,7 @@ __device__ __forceinline__ void step2_tile(const StepArgs& a, uint64_t tile, uin
         static_assert(!(F & SF_CNT), "the count reads T1's outputs before the middle factor");
         static_assert(PL::NLEV > 1, "T2 exchanges after its first level");
         static_assert(!(STAGED && (F & SF_NOPREBAR)), "a staged tile's buffer needs the barrier");
-        fs_levels<PL, 0, INV1, false, !(F & SF_NOPREBAR)>(v, sm, t, q, tw);
+        fs_levels<PL, 0, INV1, false, !(F & SF_NOPREBAR)>(v, sm, pt, tw);
         constexpr int LR = PL::lr(PL::NLEV - 1);
         constexpr int R = 1 << LR;
         constexpr int G = PL::EPT / R;
@@ -466,7 +508,7 @@ __device__ __forceinline__ void step2_tile(const StepArgs& a, uint64_t tile, uin
 #pragma unroll
             for (int j = 0; j < R; j++) v[g * R + j] = y[j];
         }
-        __syncthreads();  // every thread finished reading T1's last level
+        pt.bar();  // every thread (of the group) finished reading T1's last level
 #pragma unroll
         for (int g = 0; g < G; g++)
 #pragma unroll
@@ -475,8 +517,8 @@ __device__ __forceinline__ void step2_tile(const StepArgs& a, uint64_t tile, uin
                 sm[(size_t)(c0[g] + ((uint32_t)bitrev(r, LR) << SH)) * PL::Q4 + q] =
                     make_uint4(x.c[0], x.c[1], x.c[2], x.c[3]);
             }
-        __syncthreads();
-        fs_levels<PL, 1, INV2, true>(v, sm, t, q, tw);
+        pt.bar();
+        fs_levels<PL, 1, INV2, true, true>(v, sm, pt, tw);
         fs_last_store<PL, INV2, true, ST_KEEP, F>(v, t, a, p);
         return;
     }
@@ -653,14 +695,15 @@ __device__ __forceinline__ void pipe_pass(const PipeArgs& pa, uint32_t c, uint32
                                           const Tw* __restrict__ tw, const Tw* __restrict__ tw_lo) {
     const StepArgs x = pipe_args<PH>(pa, c);
     if constexpr (PH == 0) {
-        step_tile<L1, true, SHAPE, false, true, STAGED0, STAGED0 ? SF_EXT_A : (SF_EXT_A | SF_NOPREBAR)>(
-            x, tile, sm, tid, tw, tw_lo);
+        step_tile<L1, true, SHAPE, false, true, STAGED0,
+                  STAGED0 ? SF_EXT_A : (SF_EXT_A | SF_NOPREBAR | SF_PASS_GROUPS)>(x, tile, sm, tid, tw, tw_lo);
     } else if constexpr (PH == 1) {
         unsigned long long cnt = 0;
-        step2_tile<L2, true, false, SHAPE, true, true, false, SF_EXT_M | SF_NOPREBAR>(x, tile, sm, tid, tw, tw_lo,
-                                                                                    cnt);
+        step2_tile<L2, true, false, SHAPE, true, true, false, SF_EXT_M | SF_NOPREBAR | SF_PASS_GROUPS>(
+            x, tile, sm, tid, tw, tw_lo, cnt);
     } else {
-        step_tile<L1, false, SHAPE, true, false, false, SF_EXT_B | SF_NOPREBAR>(x, tile, sm, tid, tw, tw_lo);
+        step_tile<L1, false, SHAPE, true, false, false, SF_EXT_B | SF_NOPREBAR | SF_PASS_GROUPS>(x, tile, sm, tid,
+                                                                                              tw, tw_lo);
     }
 }
 
