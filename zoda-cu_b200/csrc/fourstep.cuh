@@ -333,11 +333,15 @@ struct FacTw {
 // A thread's quad q (of the tile's Q4) and row group t; with SF_GROUPS, half g of
 // the CTA (threads g*T/2 .. ) owns quads g*Q4/2 .. (g+1)*Q4/2 - 1, each half a
 // whole number of warps.
+#ifndef ZB_PASS_NGROUPS
+#define ZB_PASS_NGROUPS 2
+#endif
 template <class PL, int F>
 struct PassThread {
     static constexpr bool GROUPS = (F & SF_GROUPS) != 0;
-    static constexpr int GS = GROUPS ? PL::THREADS / 2 : PL::THREADS;  // threads of a barrier group
-    static constexpr int GQ = GROUPS ? PL::Q4 / 2 : PL::Q4;            // quads of a group
+    static constexpr int NG = GROUPS ? ZB_PASS_NGROUPS : 1;
+    static constexpr int GS = PL::THREADS / NG;  // threads of a barrier group
+    static constexpr int GQ = PL::Q4 / NG;       // quads of a group
     static_assert(!GROUPS || (GS % 32 == 0 && GQ >= 1 && GS % GQ == 0), "halves of whole warps and quads");
     int q, t, grp;
     __device__ __forceinline__ explicit PassThread(int tid) {
@@ -347,7 +351,7 @@ struct PassThread {
         t = l / GQ;
     }
     // the barrier between exchange writes and reads: the group's named barrier
-    // (ids 1 and 2), or the whole CTA's
+    // (ids 1 .. NG), or the whole CTA's
     __device__ __forceinline__ void bar() const {
         if constexpr (GROUPS) group_bar(1 + grp, GS);
         else __syncthreads();
