@@ -46,10 +46,11 @@ __device__ __forceinline__ void bfly4(V4& a, V4& b, uint32_t w, uint32_t ws) {
 #pragma unroll
     for (int c = 0; c < 4; c++) dif_bfly(a.c[c], b.c[c], w, ws);
 }
-template <int LH = 0>
+// FM: bit s set = the twiddle-free butterflies of stages with span 2^s use IMAD
+template <int LH = 0, int FM = ZB_FREE_IMAD_MASK>
 __device__ __forceinline__ void bfly4_1(V4& a, V4& b) {
 #pragma unroll
-    for (int c = 0; c < 4; c++) dif_bfly1<((ZB_FREE_IMAD_MASK >> LH) & 1) != 0>(a.c[c], b.c[c]);
+    for (int c = 0; c < 4; c++) dif_bfly1<((FM >> LH) & 1) != 0>(a.c[c], b.c[c]);
 }
 __device__ __forceinline__ void mul4(V4& a, const Tw t) {
 #pragma unroll
@@ -57,13 +58,13 @@ __device__ __forceinline__ void mul4(V4& a, const Tw t) {
 }
 
 namespace detail {
-template <bool INV, int LH, int J>
+template <bool INV, int LH, int J, int FM>
 __device__ __forceinline__ void bfly_at(V4* x) {
     constexpr int h = 1 << LH;
     if constexpr ((J & h) == 0) {
         constexpr int e = J & (h - 1);
         if constexpr (e == 0) {
-            bfly4_1<LH>(x[J], x[J + h]);
+            bfly4_1<LH, FM>(x[J], x[J + h]);
         } else {
             constexpr uint32_t w = root_pow(LH + 1, (uint32_t)e, INV);
             constexpr uint32_t ws = shoup(w);
@@ -71,25 +72,25 @@ __device__ __forceinline__ void bfly_at(V4* x) {
         }
     }
 }
-template <bool INV, int LH, int... Js>
+template <bool INV, int LH, int FM, int... Js>
 __device__ __forceinline__ void stage(V4* x, std::integer_sequence<int, Js...>) {
-    (bfly_at<INV, LH, Js>(x), ...);
+    (bfly_at<INV, LH, Js, FM>(x), ...);
 }
 // stages with span 2^LH down to 2^LOW
-template <bool INV, int LOG_R, int LH, int LOW = 0>
+template <bool INV, int LOG_R, int LH, int LOW = 0, int FM = ZB_FREE_IMAD_MASK>
 __device__ __forceinline__ void stages(V4* x) {
     if constexpr (LH >= LOW) {
-        stage<INV, LH>(x, std::make_integer_sequence<int, (1 << LOG_R)>{});
-        stages<INV, LOG_R, LH - 1, LOW>(x);
+        stage<INV, LH, FM>(x, std::make_integer_sequence<int, (1 << LOG_R)>{});
+        stages<INV, LOG_R, LH - 1, LOW, FM>(x);
     }
 }
 }  // namespace detail
 
 // In-register DIF DFT of size 2^LOG_R over x[0..2^LOG_R), four columns at once.
 // INV selects omega^-1 (the transform src/ntt/cpu.rs:48-60 runs before its n^-1 scale).
-template <int LOG_R, bool INV>
+template <int LOG_R, bool INV, int FM = ZB_FREE_IMAD_MASK>
 __device__ __forceinline__ void dft_dif(V4* x) {
-    detail::stages<INV, LOG_R, LOG_R - 1>(x);
+    detail::stages<INV, LOG_R, LOG_R - 1, 0, FM>(x);
 }
 
 namespace detail {
@@ -124,9 +125,9 @@ __device__ __forceinline__ void last_stage_twout(V4* x, const TwF& twf, std::int
 // k2 = bitrev(r) by twf.get<k2>(); a + b and a - b + p lie in [0, 2p), valid
 // Shoup inputs, so those sums are never reduced on their own. With SKIP0 the
 // output k2 = 0 has factor 1 and is only reduced.
-template <int LR, bool INV, bool SKIP0, class TwF>
+template <int LR, bool INV, bool SKIP0, int FM = ZB_FREE_IMAD_MASK, class TwF>
 __device__ __forceinline__ void dft_dif_twout(V4* x, const TwF& twf) {
-    if constexpr (LR > 1) detail::stages<INV, LR, LR - 1, 1>(x);
+    if constexpr (LR > 1) detail::stages<INV, LR, LR - 1, 1, FM>(x);
     detail::last_stage_twout<LR, SKIP0>(x, twf, std::make_integer_sequence<int, (1 << LR) / 2>{});
 }
 
