@@ -87,14 +87,14 @@ __device__ __forceinline__ void dif_bfly(uint32_t& a, uint32_t& b, uint32_t w, u
     a = x;
     b = y;
 }
-// Twiddle-free DIF butterfly: (a, b) -> (a + b, a - b). The unreduced sum and
-// difference are formed with IMAD (x*1 + y, x*(2^32-1) + y) so this butterfly
-// loads the FMA pipe as much as the ALU pipe: the twiddled butterflies are
-// ALU-light, these would otherwise be ALU-only and the ALU pipe would bind.
-// The multipliers 1 and 2^32-1 live in constant memory, which the assembler
-// cannot see through, so it keeps the IMADs instead of rewriting them as adds.
-// ZB_FREE_IMAD_MASK bit s set: the twiddle-free butterflies of DIF stages with
-// span 2^s use the IMAD form, else IADD3 (ALU) adds.
+// Twiddle-free DIF butterfly: (a, b) -> (a + b, a - b). Two forms of the
+// unreduced sum and difference: IADD3 adds on the ALU pipe, or IMAD
+// (x*1 + y, x*(2^32-1) + y), which moves that work to the FMA pipe (the
+// multipliers 1 and 2^32-1 live in constant memory, which the assembler cannot
+// see through, so it keeps the IMADs instead of rewriting them as adds). Each
+// kernel family picks the form per DIF stage with a mask: bit s set = the
+// butterflies of stages with span 2^s use IMAD. ZB_FREE_IMAD_MASK is the
+// default (the four-step passes); the TMA-staged kernels pass their own.
 #ifndef ZB_FREE_IMAD_MASK
 #define ZB_FREE_IMAD_MASK 0xFF
 #endif
