@@ -305,3 +305,31 @@ def test_long_recover_detects_inconsistent_rows(ctx):
     assert np.array_equal(from_dev(out), data)
     code[known[7], 3] = (int(code[known[7], 3]) + 1) % P
     assert ctx.recover(to_dev(code), known, k, cols, out, check=True) > 0
+
+
+def test_pipelined_plan_on_concurrent_streams(ctx):
+    # Pipelined launches on different streams share the context's work-queue
+    # counters; each waits for the one before (an event), so launches queued on
+    # four streams at once, on four different squares, all come out right.
+    side, cols = 2048, 8192 + 36
+    ctx.plan_set(side, {"impl": 3, "sched": 0, "l2_promo": 3, "blocked": 1, "stagger": 1, "radix": 8, "ctas": 4})
+    try:
+        ins = [rand_dev(side, cols, seed=100 + i) for i in range(4)]
+        wants = []
+        for d_in in ins:  # the single-pass TMA plan, pinned to the oracle by the tests above
+            w = torch.empty((2 * side, cols), dtype=torch.int32, device="cuda")
+            ctx.set_impl(2)
+            ctx.extend(d_in, w, side, cols)
+            wants.append(w)
+        ctx.set_impl(0)
+        outs = [torch.full((2 * side, cols), -1, dtype=torch.int32, device="cuda") for _ in ins]
+        streams = [torch.cuda.Stream() for _ in ins]
+        torch.cuda.synchronize()  # inputs, references and filled outputs are ready before the other streams run
+        for st, d_in, d_out in zip(streams, ins, outs):
+            ctx.extend(d_in, d_out, side, cols, stream=st)
+        torch.cuda.synchronize()
+        for d_out, w in zip(outs, wants):
+            assert torch.equal(d_out, w)
+    finally:
+        ctx.set_impl(0)
+        ctx.plan_clear()
