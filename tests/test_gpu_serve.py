@@ -28,19 +28,22 @@ def as_u32(t):
 def test_results_same_alone_and_in_the_mix(ctx):
     import zoda_b200
     rng = np.random.default_rng(11)
-    sides = [int(2 ** rng.integers(5, 12)) for _ in range(48)]
+    # three large squares first (about 1.4 ms of GPU work each) fill the server's
+    # three launch slots, so the burst behind them waits and is batched whatever
+    # the host's speed; then 48 squares of random sides
+    sides = [2048] * 3 + [int(2 ** rng.integers(5, 12)) for _ in range(48)]
     inputs = []
-    for s in sides:
-        cols = 4 * int(rng.integers(1, 1 + 262144 // (4 * s)))
+    for i, s in enumerate(sides):
+        cols = 131072 if i < 3 else 4 * int(rng.integers(1, 1 + 262144 // (4 * s)))
         inputs.append(torch.randint(0, P, (s, cols), dtype=torch.int64, device="cuda").to(torch.int32))
     torch.cuda.synchronize()
-    srv = zoda_b200.Server(ctx, budget_bytes=1 << 30, max_inflight=3, max_batch=16)
+    srv = zoda_b200.Server(ctx, budget_bytes=8 << 30, max_inflight=3, max_batch=16)
     tickets = [None] * len(sides)
 
     def producer():  # a burst (more requests than streams), then Poisson-like arrivals
         for i, (s, a) in enumerate(zip(sides, inputs)):
             tickets[i] = srv.submit(a, s, a.shape[1])
-            if i >= 24:
+            if i >= 27:
                 time.sleep(float(rng.exponential(0.0005)))
 
     th = threading.Thread(target=producer)
