@@ -122,14 +122,17 @@ static void build_side_tables(int ls, int lept, std::vector<Tw>& all, size_t off
     off[6] = all.size();
 }
 
-// Copies input row m to output row 2m for every m on a few host threads, from
+// Copies columns [0, ncopy) of every input row m to output row 2m on host
+// threads (one per ZB_HOST_COPY_DIV hardware threads, 1 … 16), from
 // construction until join() (or destruction, on an early error return).
-// Copies columns [0, ncopy) of every input row m to output row 2m on host threads.
+#ifndef ZB_HOST_COPY_DIV
+#define ZB_HOST_COPY_DIV 2
+#endif
 class EvenRowCopy {
    public:
     EvenRowCopy(const uint32_t* in, uint32_t* out, uint32_t k, uint64_t cols, uint64_t ncopy) {
         if (ncopy == 0) return;
-        unsigned n = std::thread::hardware_concurrency() / 2;
+        unsigned n = std::thread::hardware_concurrency() / ZB_HOST_COPY_DIV;
         n = n < 1 ? 1 : n > 16 ? 16 : n;
         if (n > k) n = k;
         for (unsigned t = 0; t < n; t++)
@@ -150,7 +153,10 @@ class EvenRowCopy {
 
 // Share of the column chunks of a host call whose even output rows return
 // over PCIe rather than through the host copy (measured on B200 hosts).
-constexpr double HOST_EVEN_DEVICE_SHARE = 0.125;
+#ifndef ZB_HOST_EVEN_SHARE
+#define ZB_HOST_EVEN_SHARE 0.125
+#endif
+constexpr double HOST_EVEN_DEVICE_SHARE = ZB_HOST_EVEN_SHARE;
 
 // A wait that nothing completes: the bounded wait gives up and flags it.
 __global__ void k_selftest_wait(int* __restrict__ err) {
