@@ -158,6 +158,11 @@ class EvenRowCopy {
 #endif
 constexpr double HOST_EVEN_DEVICE_SHARE = ZB_HOST_EVEN_SHARE;
 
+// Input bytes per column chunk of a host call (at most MAX_CHUNKS chunks).
+#ifndef ZB_HOST_CHUNK_MIB
+#define ZB_HOST_CHUNK_MIB 64
+#endif
+
 // A wait that nothing completes: the bounded wait gives up and flags it.
 __global__ void k_selftest_wait(int* __restrict__ err) {
     __shared__ uint64_t bar;
@@ -414,8 +419,8 @@ zoda_status zoda_extend_host(zoda_ctx* ctx, const uint32_t* h_in, uint32_t* h_ou
     // Column chunks of ~64 MiB input rotate over NHS streams, so the upload of
     // one chunk, the kernel of another and the download of a third overlap
     // (the two copy directions run on separate engines).
-    const uint64_t in_bytes = (uint64_t)k * cols * 4;
-    uint64_t nch = (in_bytes + (64ull << 20) - 1) / (64ull << 20);
+    const uint64_t in_bytes = (uint64_t)k * cols * 4, chunk_bytes = (uint64_t)ZB_HOST_CHUNK_MIB << 20;
+    uint64_t nch = (in_bytes + chunk_bytes - 1) / chunk_bytes;
     if (nch > (uint64_t)zoda_ctx::MAX_CHUNKS) nch = zoda_ctx::MAX_CHUNKS;
     if (nch > cols / 4) nch = cols / 4 ? cols / 4 : 1;
     uint64_t cw = (cols + nch - 1) / nch;

@@ -91,9 +91,15 @@ struct zoda_ctx {
     bool planned[13] = {};
     // host-call staging: NHS streams, one input and one output buffer each, and
     // 4 timing events per chunk for up to MAX_CHUNKS chunks
-    static constexpr int NHS = 3;
-    static constexpr int MAX_CHUNKS = 64;
-    cudaStream_t hs[NHS] = {nullptr, nullptr, nullptr};
+#ifndef ZB_HOST_STREAMS
+#define ZB_HOST_STREAMS 3
+#endif
+#ifndef ZB_HOST_MAX_CHUNKS
+#define ZB_HOST_MAX_CHUNKS 64
+#endif
+    static constexpr int NHS = ZB_HOST_STREAMS;
+    static constexpr int MAX_CHUNKS = ZB_HOST_MAX_CHUNKS;
+    cudaStream_t hs[NHS] = {};
     zb::DevBuf hin[NHS], hout[NHS];
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t cev[MAX_CHUNKS][4] = {};
