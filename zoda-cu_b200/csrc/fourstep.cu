@@ -306,6 +306,9 @@ zoda_status pipe_t(const zoda_ctx* ctx, const StepArgs pass[3], uint64_t cols, c
     zoda_ctx* mc = const_cast<zoda_ctx*>(ctx);  // the pipeline's counters and ordering event
     std::lock_guard<std::mutex> lock(mc->pipe_mu);
     const size_t cbytes = (size_t)(1 + 2 * nch) * sizeof(uint32_t);
+    // a larger square replaces the counters: the launch before, on whatever
+    // stream, finishes with the old ones first
+    if (mc->pipe_done && cbytes > mc->pipe_cnt.bytes) ZB_CUDA(cudaEventSynchronize(mc->pipe_done));
     zoda_status s = mc->pipe_cnt.ensure(cbytes);
     if (s != ZODA_OK) return s;
     if (!mc->pipe_done) ZB_CUDA(cudaEventCreateWithFlags(&mc->pipe_done, cudaEventDisableTiming));
